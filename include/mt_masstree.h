@@ -1,0 +1,135 @@
+/*
+ * C ABI of the B200 masstree (libmt_b200.so).
+ *
+ * Drop-in boundary for IndexinGPU's gpu_masstree host API
+ * (include/gpu_masstree.hpp:84-191 of the reference).  Every entry point takes
+ * plain pointers and sizes; key and value buffers are flat uint32 "slice"
+ * arrays of stride max_key_length / max_value_length (reference README.md:43-50)
+ * and may live in device memory or in pinned host memory mapped into the
+ * device address space.  A NULL length array means "every item has the maximum
+ * length".  value_lengths[i] == 0 after a find means "not found".
+ *
+ * Calls are asynchronous on `stream` (a cudaStream_t passed as void*).  A tree
+ * must be driven from one stream at a time (the reference has the same rule:
+ * kernels on one reclaimer must not overlap, simple_debra_reclaim.hpp:189,226).
+ * Device-side failures (pool exhausted, lock timeout, corruption) are recorded
+ * on the device and returned by mt_sync().
+ */
+#ifndef MT_MASSTREE_H_
+#define MT_MASSTREE_H_
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mt_masstree mt_masstree;
+
+/* Status codes. */
+enum {
+  MT_OK = 0,
+  MT_ERR_OOM = 1,          /* slab pool exhausted */
+  MT_ERR_LOCK_TIMEOUT = 2, /* a node lock was not obtained within the bound */
+  MT_ERR_CORRUPT = 3,      /* an invalid slab index or a runaway traversal was seen */
+  MT_ERR_INVALID_ARG = 4,
+  MT_ERR_CUDA = 5,
+  MT_ERR_RETRY_LIMIT = 6,  /* an insert restarted its descent too often */
+  MT_ERR_KEY_TOO_LONG = 7  /* scan depth beyond the scan frame capacity */
+};
+
+/* Request kinds of mt_mixed_batch (reference macros.hpp:51-57). */
+enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 };
+
+/* Flags. */
+#define MT_FLAG_CONCURRENT 1u       /* find/scan may run beside writers (reference template `concurrent`) */
+#define MT_FLAG_UPDATE_IF_EXISTS 2u /* insert overwrites an existing key (reference `update_if_exists`) */
+#define MT_FLAG_USE_UPPER_KEY 4u    /* scan stops after upper_keys (reference `use_upper_key`) */
+
+typedef struct mt_stats_t {
+  uint64_t total_slabs;     /* slabs in the pool (128 bytes each) */
+  uint64_t used_slabs;      /* handed out and not yet returned */
+  uint64_t free_slabs;      /* never used or returned */
+  uint64_t limbo_slabs;     /* retired, returned at the next call on the tree */
+  uint32_t num_shards;
+  uint32_t tile_size;
+  uint32_t device_error;    /* first device error since the last mt_sync */
+  uint32_t device_error_count;
+} mt_stats_t;
+
+/* Construction.  Replaces gpu_masstree(allocator(pool_ratio), reclaimer())
+ * (reference gpu_masstree.hpp:67-72, simple_slab_alloc.hpp:56-69): the slab
+ * pool takes pool_ratio of the currently free device memory.  tile_size is the
+ * number of lanes serving one request (4, 8, 16 or 32). */
+int mt_create(mt_masstree** out, float pool_ratio, uint32_t tile_size);
+/* Same, with the pool size given in bytes. */
+int mt_create_bytes(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size);
+/* Reference ~gpu_masstree / ~simple_slab_allocator (gpu_masstree.hpp:80-82). */
+int mt_destroy(mt_masstree* tree);
+
+/* Launch shape: lanes per request (4/8/16/32) and resident blocks per SM
+ * (0 = as many as fit).  New in this library. */
+int mt_set_tile_size(mt_masstree* tree, uint32_t tile_size);
+int mt_set_blocks_per_sm(mt_masstree* tree, uint32_t blocks_per_sm);
+
+/* Reference gpu_masstree::find (gpu_masstree.hpp:86-99). */
+int mt_find(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
+            uint32_t* values, uint32_t max_value_length, uint32_t* value_lengths, uint32_t num_keys,
+            uint32_t flags, void* stream);
+
+/* Reference gpu_masstree::insert (gpu_masstree.hpp:101-115).  results may be
+ * NULL (the reference has none); else results[i] = inserted (or updated). */
+int mt_insert(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
+              const uint32_t* values, uint32_t max_value_length, const uint32_t* value_lengths,
+              uint32_t num_keys, bool* results, uint32_t flags, void* stream);
+
+/* Reference gpu_masstree::update (gpu_masstree.hpp:117-130). */
+int mt_update(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
+              const uint32_t* values, uint32_t max_value_length, const uint32_t* value_lengths,
+              uint32_t num_keys, bool* results, uint32_t flags, void* stream);
+
+/* Reference gpu_masstree::erase (gpu_masstree.hpp:132-145). */
+int mt_erase(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
+             uint32_t num_keys, bool* results, uint32_t flags, void* stream);
+
+/* Reference gpu_masstree::scan (gpu_masstree.hpp:147-171).  Query q writes
+ * counts[q], values[q][max_count][max_value_length], value_lengths[q][max_count],
+ * out_keys[q][max_count][max_key_length], out_key_lengths[q][max_count]; every
+ * output pointer may be NULL.  Both bounds are inclusive. */
+int mt_scan(mt_masstree* tree, const uint32_t* lower_keys, const uint32_t* lower_key_lengths,
+            uint32_t max_key_length, uint32_t max_count_per_query, uint32_t num_queries,
+            const uint32_t* upper_keys, const uint32_t* upper_key_lengths, uint32_t* counts,
+            uint32_t* values, uint32_t max_value_length, uint32_t* value_lengths,
+            uint32_t* out_keys, uint32_t* out_key_lengths, uint32_t flags, void* stream);
+
+/* Reference gpu_masstree::mixed_batch (gpu_masstree.hpp:173-191): request_types
+ * uses MT_REQ_*; values / value_lengths are inputs for insert and update and
+ * outputs for find; results[i] (may be NULL) is written for insert, update and
+ * erase. */
+int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32_t* keys,
+                   uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
+                   uint32_t max_value_length, uint32_t* value_lengths, bool* results,
+                   uint32_t num_requests, uint32_t flags, void* stream);
+
+/* Wait for `stream`, then return (and clear) the first device error recorded
+ * since the previous mt_sync (MT_OK if none). */
+int mt_sync(mt_masstree* tree, void* stream);
+
+/* Pool statistics (synchronous; reference simple_slab_allocator::print_stats,
+ * simple_slab_alloc.hpp:82-89). */
+int mt_stats(mt_masstree* tree, mt_stats_t* out);
+
+/* Return retired slabs to the free lists now (normally done at the start of
+ * every call).  Retired slabs are those unlinked by earlier calls. */
+int mt_reclaim(mt_masstree* tree, void* stream);
+
+/* Human-readable name of a status code. */
+const char* mt_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MT_MASSTREE_H_ */

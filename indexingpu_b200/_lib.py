@@ -1,0 +1,63 @@
+"""ctypes binding of libmt_b200.so (declarations mirror include/mt_masstree.h)."""
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libmt_b200.so")
+
+_u32 = ctypes.c_uint32
+_u64 = ctypes.c_uint64
+_p = ctypes.c_void_p
+_int = ctypes.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "mt_create": (_int, [ctypes.POINTER(_p), ctypes.c_float, _u32]),
+    "mt_create_bytes": (_int, [ctypes.POINTER(_p), _u64, _u32]),
+    "mt_destroy": (_int, [_p]),
+    "mt_set_tile_size": (_int, [_p, _u32]),
+    "mt_set_blocks_per_sm": (_int, [_p, _u32]),
+    "mt_find": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _u32, _p]),
+    "mt_insert": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),
+    "mt_update": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),
+    "mt_erase": (_int, [_p, _p, _u32, _p, _u32, _p, _u32, _p]),
+    "mt_scan": (_int, [_p, _p, _p, _u32, _u32, _u32, _p, _p, _p, _p, _u32, _p, _p, _p, _u32, _p]),
+    "mt_mixed_batch": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _u32, _p]),
+    "mt_sync": (_int, [_p, _p]),
+    "mt_stats": (_int, [_p, _p]),
+    "mt_reclaim": (_int, [_p, _p]),
+    "mt_status_string": (ctypes.c_char_p, [_int]),
+}
+
+
+class MtStats(ctypes.Structure):
+    _fields_ = [
+        ("total_slabs", _u64),
+        ("used_slabs", _u64),
+        ("free_slabs", _u64),
+        ("limbo_slabs", _u64),
+        ("num_shards", _u32),
+        ("tile_size", _u32),
+        ("device_error", _u32),
+        ("device_error_count", _u32),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m indexingpu_b200.build` "
+                "(there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

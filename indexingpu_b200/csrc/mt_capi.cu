@@ -1,0 +1,535 @@
+// Batch kernels and the C ABI of libmt_b200.so.
+//
+// Every host call is one stream-ordered launch of a persistent grid-stride
+// kernel (the reference's batch_kernel, include/kernels.hpp:31-103), preceded by
+// the reclaim pass that returns slabs retired by earlier calls.  Differences:
+//   * the launch shape (blocks per SM from the occupancy API, SM count) is
+//     computed once per kernel and cached, not on every call (the reference
+//     queries it per call, kernels.hpp:91-99);
+//   * a tile serves T requests per round, loading their metadata coalesced
+//     (one request per lane) and writing results coalesced;
+//   * there is no block-wide barrier per round: reclamation is launch-granular
+//     (see mt_pool.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <unordered_map>
+
+#include "mt_tree.cuh"
+#include "../../include/mt_masstree.h"
+
+namespace mtb {
+
+constexpr int kBlock = 128;
+constexpr uint32_t kShards = 64;
+constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
+
+enum op_kind : int { OP_FIND = 0, OP_INSERT = 1, OP_UPSERT = 2, OP_UPDATE = 3, OP_ERASE = 4, OP_MIXED = 5 };
+
+struct batch_args {
+  const uint8_t* types;
+  const uint32_t* keys;
+  const uint32_t* key_lengths;
+  uint32_t* values;              // insert/update: input, find: output
+  const uint32_t* value_lengths_in;
+  uint32_t* value_lengths_out;
+  bool* results;
+  uint32_t max_key_length;
+  uint32_t max_value_length;
+  uint32_t n;
+};
+
+struct scan_args {
+  const uint32_t* lower;
+  const uint32_t* lower_lengths;
+  const uint32_t* upper;
+  const uint32_t* upper_lengths;
+  uint32_t* counts;
+  uint32_t* values;
+  uint32_t* value_lengths;
+  uint32_t* out_keys;
+  uint32_t* out_key_lengths;
+  scan_frame* frames;
+  uint32_t max_key_length;
+  uint32_t max_value_length;
+  uint32_t max_count;
+  uint32_t n;
+  uint32_t use_upper;
+};
+
+// One request of any kind, executed by the whole tile.
+template <int T, int OP, bool CONC>
+MT_DEV void run_request(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const batch_args& a,
+                        uint32_t j, uint32_t kind, uint32_t klen, uint32_t vlen, uint32_t& res, uint32_t& vout) {
+  const uint32_t* key = a.keys + (size_t)j * a.max_key_length;
+  if (kind == MT_REQ_FIND) {
+    uint32_t* out = a.values ? a.values + (size_t)j * a.max_value_length : nullptr;
+    const uint32_t l = coop_find<T, CONC>(t, tv, key, klen, out, a.max_value_length);
+    vout = l;
+  } else if (kind == MT_REQ_INSERT) {
+    const uint32_t* val = a.values + (size_t)j * a.max_value_length;
+    const int r = (OP == OP_UPSERT) ? coop_insert<T, true>(t, tv, cache, key, klen, val, vlen)
+                                    : coop_insert<T, false>(t, tv, cache, key, klen, val, vlen);
+    res = (r == R_OK) ? 1u : 0u;
+  } else if (kind == MT_REQ_UPDATE) {
+    const uint32_t* val = a.values + (size_t)j * a.max_value_length;
+    res = (coop_update<T>(t, tv, cache, key, klen, val, vlen) == R_OK) ? 1u : 0u;
+  } else {
+    res = (coop_erase<T>(t, tv, key, klen) == R_OK) ? 1u : 0u;
+  }
+}
+
+template <int T, int OP, bool CONC>
+__global__ void __launch_bounds__(kBlock) batch_kernel(tree_view tv, batch_args a) {
+  tile<T> t;
+  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
+  const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
+  slab_cache<T> cache;
+  cache.init(tv.pool, tile_id);
+  for (uint32_t base = tile_id * T; base < a.n; base += num_tiles * T) {
+    if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
+    const uint32_t i = base + t.rank;
+    const bool valid = i < a.n;
+    uint32_t kind = 0, klen = 0, vlen = 0;
+    if (valid) {
+      if constexpr (OP == OP_MIXED) kind = a.types[i];
+      else if constexpr (OP == OP_FIND) kind = MT_REQ_FIND;
+      else if constexpr (OP == OP_INSERT || OP == OP_UPSERT) kind = MT_REQ_INSERT;
+      else if constexpr (OP == OP_UPDATE) kind = MT_REQ_UPDATE;
+      else kind = MT_REQ_ERASE;
+      klen = a.key_lengths ? a.key_lengths[i] : a.max_key_length;
+      if (kind == MT_REQ_INSERT || kind == MT_REQ_UPDATE)
+        vlen = a.value_lengths_in ? a.value_lengths_in[i] : a.max_value_length;
+    }
+    // Lengths beyond the row stride (or unknown kinds) would read outside the
+    // caller's buffers: such requests are skipped and reported.
+    const bool bad = valid && (klen > a.max_key_length || vlen > a.max_value_length || kind > MT_REQ_UPDATE);
+    if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
+    uint32_t res = 0, vout = 0;
+    const uint32_t nreq = min((uint32_t)T, a.n - base);
+    for (uint32_t r = 0; r < nreq; ++r) {
+      if (t.shfl((uint32_t)bad, (int)r)) continue;
+      const uint32_t k = t.shfl(kind, (int)r);
+      const uint32_t kl = t.shfl(klen, (int)r);
+      const uint32_t vl = t.shfl(vlen, (int)r);
+      uint32_t rr = 0, vo = 0;
+      run_request<T, OP, CONC>(t, tv, cache, a, base + r, k, kl, vl, rr, vo);
+      if (t.rank == r) { res = rr; vout = vo; }
+    }
+    if (valid) {
+      if (kind == MT_REQ_FIND) {
+        if (a.value_lengths_out) a.value_lengths_out[i] = vout;
+      } else if (a.results) {
+        a.results[i] = res != 0u;
+      }
+    }
+  }
+  cache.release(t, tv.pool);
+}
+
+template <int T, bool CONC>
+__global__ void __launch_bounds__(kBlock) scan_kernel(tree_view tv, scan_args a) {
+  tile<T> t;
+  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
+  const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
+  scan_frame* frames = a.frames + (size_t)tile_id * kScanDepth;
+  for (uint32_t base = tile_id * T; base < a.n; base += num_tiles * T) {
+    if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
+    const uint32_t i = base + t.rank;
+    uint32_t llen = 0, ulen = 0, cnt = 0;
+    if (i < a.n) {
+      llen = a.lower_lengths ? a.lower_lengths[i] : a.max_key_length;
+      ulen = a.upper_lengths ? a.upper_lengths[i] : a.max_key_length;
+    }
+    const bool bad = i < a.n && (llen > a.max_key_length || (a.use_upper && ulen > a.max_key_length));
+    if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
+    const uint32_t nreq = min((uint32_t)T, a.n - base);
+    for (uint32_t r = 0; r < nreq; ++r) {
+      if (t.shfl((uint32_t)bad, (int)r)) continue;
+      const uint32_t q = base + r;
+      const uint32_t ll = t.shfl(llen, (int)r);
+      const uint32_t ul = t.shfl(ulen, (int)r);
+      scan_out o;
+      const size_t mc = a.max_count;
+      o.values = a.values ? a.values + (size_t)q * mc * a.max_value_length : nullptr;
+      o.value_lengths = a.value_lengths ? a.value_lengths + (size_t)q * mc : nullptr;
+      o.maxV = a.max_value_length;
+      o.keys = a.out_keys ? a.out_keys + (size_t)q * mc * a.max_key_length : nullptr;
+      o.key_lengths = a.out_key_lengths ? a.out_key_lengths + (size_t)q * mc : nullptr;
+      o.maxK = a.max_key_length;
+      const uint32_t* lower = a.lower + (size_t)q * a.max_key_length;
+      const uint32_t* upper = a.upper ? a.upper + (size_t)q * a.max_key_length : nullptr;
+      const uint32_t c = coop_scan<T, CONC>(t, tv, lower, ll, a.use_upper != 0u && upper != nullptr, upper, ul,
+                                           a.max_count, o, frames, kScanDepth);
+      if (t.rank == r) cnt = c;
+    }
+    if (i < a.n && a.counts) a.counts[i] = cnt;
+  }
+}
+
+// Return slabs retired by earlier launches to their shard's free stack.
+__global__ void reclaim_kernel(pool_view p) {
+  for (uint32_t s = blockIdx.x; s < p.num_shards; s += gridDim.x) {
+    __shared__ int top, n;
+    if (threadIdx.x == 0) {
+      top = max(*p.top(s), 0);
+      n = *p.limbo_count(s);
+      if (top + n > (int)p.shard_slabs) {
+        record_error(p, ERR_CORRUPT);
+        n = 0;
+      }
+    }
+    __syncthreads();
+    uint32_t* stack = p.free_stack + (size_t)s * p.shard_slabs;
+    const uint32_t* limbo = p.limbo + (size_t)s * p.shard_slabs;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) stack[top + i] = limbo[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      *p.top(s) = top + n;
+      *p.limbo_count(s) = 0;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace mtb
+
+// ------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------
+
+using namespace mtb;
+
+struct mt_masstree {
+  int device = 0;
+  int sms = 0;
+  uint32_t tile_size = 8;
+  uint32_t blocks_per_sm = 0;  // 0 = occupancy limit
+  void* mem = nullptr;
+  tree_view tv{};
+  scan_frame* frames = nullptr;
+  size_t frames_tiles = 0;
+  uint32_t* h_err = nullptr;  // pinned
+};
+
+namespace {
+
+struct launch_cache {
+  std::mutex mu;
+  std::unordered_map<const void*, int> bps;
+};
+launch_cache& lcache() {
+  static launch_cache c;
+  return c;
+}
+
+int max_blocks_per_sm(const void* fn) {
+  auto& c = lcache();
+  std::lock_guard<std::mutex> g(c.mu);
+  auto it = c.bps.find(fn);
+  if (it != c.bps.end()) return it->second;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kBlock, 0) != cudaSuccess || b <= 0) b = 1;
+  c.bps.emplace(fn, b);
+  return b;
+}
+
+int grid_for(const mt_masstree* t, const void* fn) {
+  int b = max_blocks_per_sm(fn);
+  if (t->blocks_per_sm > 0) b = std::min<int>(b, (int)t->blocks_per_sm);
+  return b * t->sms;
+}
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? MT_OK : MT_ERR_CUDA; }
+
+int launch_reclaim(mt_masstree* t, cudaStream_t s) {
+  reclaim_kernel<<<kShards, 256, 0, s>>>(t->tv.pool);
+  return cuda_status(cudaGetLastError());
+}
+
+template <int T, int OP, bool CONC>
+int launch_batch_t(mt_masstree* t, const batch_args& a, cudaStream_t s) {
+  const void* fn = (const void*)batch_kernel<T, OP, CONC>;
+  const int grid = grid_for(t, fn);
+  batch_kernel<T, OP, CONC><<<grid, kBlock, 0, s>>>(t->tv, a);
+  return cuda_status(cudaGetLastError());
+}
+
+template <int OP, bool CONC>
+int launch_batch(mt_masstree* t, const batch_args& a, cudaStream_t s) {
+  if (a.n == 0) return MT_OK;
+  int rc = launch_reclaim(t, s);
+  if (rc) return rc;
+  switch (t->tile_size) {
+    case 4: return launch_batch_t<4, OP, CONC>(t, a, s);
+    case 8: return launch_batch_t<8, OP, CONC>(t, a, s);
+    case 16: return launch_batch_t<16, OP, CONC>(t, a, s);
+    case 32: return launch_batch_t<32, OP, CONC>(t, a, s);
+    default: return MT_ERR_INVALID_ARG;
+  }
+}
+
+template <int T, bool CONC>
+int launch_scan_t(mt_masstree* t, scan_args a, cudaStream_t s) {
+  const void* fn = (const void*)scan_kernel<T, CONC>;
+  const int grid = grid_for(t, fn);
+  const size_t tiles = (size_t)grid * kBlock / T;
+  if (tiles > t->frames_tiles) {
+    // Scan frames: grown on demand, kept for later calls.
+    cudaStreamSynchronize(s);
+    if (t->frames) cudaFree(t->frames);
+    t->frames = nullptr;
+    t->frames_tiles = 0;
+    if (cudaMalloc(&t->frames, tiles * kScanDepth * sizeof(scan_frame)) != cudaSuccess) return MT_ERR_CUDA;
+    t->frames_tiles = tiles;
+  }
+  a.frames = t->frames;
+  scan_kernel<T, CONC><<<grid, kBlock, 0, s>>>(t->tv, a);
+  return cuda_status(cudaGetLastError());
+}
+
+template <bool CONC>
+int launch_scan(mt_masstree* t, const scan_args& a, cudaStream_t s) {
+  switch (t->tile_size) {
+    case 4: return launch_scan_t<4, CONC>(t, a, s);
+    case 8: return launch_scan_t<8, CONC>(t, a, s);
+    case 16: return launch_scan_t<16, CONC>(t, a, s);
+    case 32: return launch_scan_t<32, CONC>(t, a, s);
+    default: return MT_ERR_INVALID_ARG;
+  }
+}
+
+bool valid_tile(uint32_t ts) { return ts == 4 || ts == 8 || ts == 16 || ts == 32; }
+
+int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
+  if (!out || !valid_tile(tile_size)) return MT_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto* t = new (std::nothrow) mt_masstree();
+  if (!t) return MT_ERR_OOM;
+  t->tile_size = tile_size;
+  if (cudaGetDevice(&t->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, t->device) != cudaSuccess) {
+    delete t;
+    return MT_ERR_CUDA;
+  }
+  // Per slab: 128 B node + 4 B free-stack entry + 4 B limbo entry.
+  uint64_t slabs = pool_bytes / (128u + 8u);
+  slabs = std::min<uint64_t>(slabs, 0xFFFFFF00ull);
+  const uint32_t shard_slabs = (uint32_t)(slabs / kShards);
+  if (shard_slabs < 64) { delete t; return MT_ERR_INVALID_ARG; }
+  const uint64_t nslabs = (uint64_t)shard_slabs * kShards;
+  const size_t slab_bytes = nslabs * 128u;
+  const size_t stack_bytes = nslabs * 4u;
+  const size_t ctr_bytes = (size_t)kShards * 3u * kCtrStride * sizeof(int);
+  const size_t err_bytes = 128;
+  const size_t total = slab_bytes + 2 * stack_bytes + ctr_bytes + err_bytes;
+  if (cudaMalloc(&t->mem, total) != cudaSuccess) { delete t; return MT_ERR_OOM; }
+  char* base = (char*)t->mem;
+  pool_view& p = t->tv.pool;
+  p.slabs = (uint32_t*)base;
+  p.free_stack = (uint32_t*)(base + slab_bytes);
+  p.limbo = (uint32_t*)(base + slab_bytes + stack_bytes);
+  p.ctr = (int*)(base + slab_bytes + 2 * stack_bytes);
+  p.err = (uint32_t*)(base + slab_bytes + 2 * stack_bytes + ctr_bytes);
+  p.num_slabs = (uint32_t)nslabs;
+  p.num_shards = kShards;
+  p.shard_slabs = shard_slabs;
+  cudaError_t e = cudaMemset(p.ctr, 0, ctr_bytes + err_bytes);
+  // Root of trie layer 0 = slab 0 (shard 0's bump pointer starts past it).
+  uint32_t root_img[32] = {0};
+  root_img[WORD_HIGH] = 0xFFFFFFFFu;
+  root_img[WORD_SIB] = kInvalid;
+  root_img[WORD_META] = META_BORDER | META_ROOT;
+  root_img[WORD_KS] = 0u;
+  const int one = 1;
+  if (e == cudaSuccess) e = cudaMemcpy(p.slabs, root_img, sizeof(root_img), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.bump(0), &one, sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMallocHost(&t->h_err, 2 * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    cudaFree(t->mem);
+    delete t;
+    return MT_ERR_CUDA;
+  }
+  t->tv.root = 0;
+  *out = t;
+  return MT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_create(mt_masstree** out, float pool_ratio, uint32_t tile_size) {
+  if (!(pool_ratio > 0.0f && pool_ratio <= 1.0f)) return MT_ERR_INVALID_ARG;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return MT_ERR_CUDA;
+  return create_impl(out, (uint64_t)((double)free_b * (double)pool_ratio), tile_size);
+}
+
+int mt_create_bytes(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
+  return create_impl(out, pool_bytes, tile_size);
+}
+
+int mt_destroy(mt_masstree* t) {
+  if (!t) return MT_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  if (t->frames) cudaFree(t->frames);
+  if (t->mem) cudaFree(t->mem);
+  if (t->h_err) cudaFreeHost(t->h_err);
+  delete t;
+  return MT_OK;
+}
+
+int mt_set_tile_size(mt_masstree* t, uint32_t ts) {
+  if (!t || !valid_tile(ts)) return MT_ERR_INVALID_ARG;
+  t->tile_size = ts;
+  return MT_OK;
+}
+
+int mt_set_blocks_per_sm(mt_masstree* t, uint32_t b) {
+  if (!t) return MT_ERR_INVALID_ARG;
+  t->blocks_per_sm = b;
+  return MT_OK;
+}
+
+int mt_find(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, uint32_t* values,
+            uint32_t maxV, uint32_t* vlens, uint32_t n, uint32_t flags, void* stream) {
+  if (!t || (n && (!keys || !vlens || maxK == 0))) return MT_ERR_INVALID_ARG;
+  batch_args a{};
+  a.keys = keys; a.key_lengths = klens; a.values = values; a.value_lengths_out = vlens;
+  a.max_key_length = maxK; a.max_value_length = values ? maxV : 0u; a.n = n;
+  cudaStream_t s = (cudaStream_t)stream;
+  return (flags & MT_FLAG_CONCURRENT) ? launch_batch<OP_FIND, true>(t, a, s) : launch_batch<OP_FIND, false>(t, a, s);
+}
+
+int mt_insert(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, const uint32_t* values,
+              uint32_t maxV, const uint32_t* vlens, uint32_t n, bool* results, uint32_t flags, void* stream) {
+  if (!t || (n && (!keys || !values || maxK == 0))) return MT_ERR_INVALID_ARG;
+  batch_args a{};
+  a.keys = keys; a.key_lengths = klens; a.values = const_cast<uint32_t*>(values); a.value_lengths_in = vlens;
+  a.results = results; a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
+  cudaStream_t s = (cudaStream_t)stream;
+  return (flags & MT_FLAG_UPDATE_IF_EXISTS) ? launch_batch<OP_UPSERT, true>(t, a, s)
+                                            : launch_batch<OP_INSERT, true>(t, a, s);
+}
+
+int mt_update(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, const uint32_t* values,
+              uint32_t maxV, const uint32_t* vlens, uint32_t n, bool* results, uint32_t flags, void* stream) {
+  (void)flags;
+  if (!t || (n && (!keys || !values || maxK == 0))) return MT_ERR_INVALID_ARG;
+  batch_args a{};
+  a.keys = keys; a.key_lengths = klens; a.values = const_cast<uint32_t*>(values); a.value_lengths_in = vlens;
+  a.results = results; a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
+  return launch_batch<OP_UPDATE, true>(t, a, (cudaStream_t)stream);
+}
+
+int mt_erase(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, uint32_t n,
+             bool* results, uint32_t flags, void* stream) {
+  (void)flags;
+  if (!t || (n && (!keys || maxK == 0))) return MT_ERR_INVALID_ARG;
+  batch_args a{};
+  a.keys = keys; a.key_lengths = klens; a.results = results; a.max_key_length = maxK; a.n = n;
+  return launch_batch<OP_ERASE, true>(t, a, (cudaStream_t)stream);
+}
+
+int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, uint32_t maxK,
+                   const uint32_t* klens, uint32_t* values, uint32_t maxV, uint32_t* vlens, bool* results,
+                   uint32_t n, uint32_t flags, void* stream) {
+  (void)flags;
+  if (!t || (n && (!types || !keys || !values || !vlens || maxK == 0 || maxV == 0))) return MT_ERR_INVALID_ARG;
+  batch_args a{};
+  a.types = types; a.keys = keys; a.key_lengths = klens; a.values = values;
+  a.value_lengths_in = vlens; a.value_lengths_out = vlens; a.results = results;
+  a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
+  return launch_batch<OP_MIXED, true>(t, a, (cudaStream_t)stream);
+}
+
+int mt_scan(mt_masstree* t, const uint32_t* lower, const uint32_t* lower_lens, uint32_t maxK, uint32_t max_count,
+            uint32_t nq, const uint32_t* upper, const uint32_t* upper_lens, uint32_t* counts, uint32_t* values,
+            uint32_t maxV, uint32_t* vlens, uint32_t* out_keys, uint32_t* out_klens, uint32_t flags,
+            void* stream) {
+  if (!t || (nq && (!lower || maxK == 0))) return MT_ERR_INVALID_ARG;
+  if ((flags & MT_FLAG_USE_UPPER_KEY) && nq && !upper) return MT_ERR_INVALID_ARG;
+  if (nq == 0) return MT_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = launch_reclaim(t, s);
+  if (rc) return rc;
+  scan_args a{};
+  a.lower = lower; a.lower_lengths = lower_lens; a.upper = upper; a.upper_lengths = upper_lens;
+  a.counts = counts; a.values = values; a.value_lengths = vlens; a.out_keys = out_keys;
+  a.out_key_lengths = out_klens; a.max_key_length = maxK; a.max_value_length = values ? maxV : 0u;
+  a.max_count = max_count; a.n = nq; a.use_upper = (flags & MT_FLAG_USE_UPPER_KEY) ? 1u : 0u;
+  return (flags & MT_FLAG_CONCURRENT) ? launch_scan<true>(t, a, s) : launch_scan<false>(t, a, s);
+}
+
+int mt_sync(mt_masstree* t, void* stream) {
+  if (!t) return MT_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(t->h_err, t->tv.pool.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return MT_ERR_CUDA;
+  const uint32_t code = t->h_err[0];
+  if (code != 0u) {
+    e = cudaMemsetAsync(t->tv.pool.err, 0, 3 * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return MT_ERR_CUDA;
+  }
+  return (int)code;
+}
+
+int mt_reclaim(mt_masstree* t, void* stream) {
+  if (!t) return MT_ERR_INVALID_ARG;
+  return launch_reclaim(t, (cudaStream_t)stream);
+}
+
+int mt_stats(mt_masstree* t, mt_stats_t* out) {
+  if (!t || !out) return MT_ERR_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return MT_ERR_CUDA;
+  const pool_view& p = t->tv.pool;
+  const size_t nctr = (size_t)p.num_shards * 3u * kCtrStride;
+  int* h = new (std::nothrow) int[nctr];
+  if (!h) return MT_ERR_OOM;
+  uint32_t err[2] = {0, 0};
+  cudaError_t e = cudaMemcpy(h, p.ctr, nctr * sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(err, p.err, sizeof(err), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) { delete[] h; return MT_ERR_CUDA; }
+  uint64_t handed = 0, stacked = 0, limbo = 0;
+  for (uint32_t s = 0; s < p.num_shards; ++s) {
+    const int top = h[(3 * s + 0) * kCtrStride];
+    const int bump = h[(3 * s + 1) * kCtrStride];
+    const int lim = h[(3 * s + 2) * kCtrStride];
+    handed += (uint64_t)std::min<int>(std::max(bump, 0), (int)p.shard_slabs);
+    stacked += (uint64_t)std::max(top, 0);
+    limbo += (uint64_t)std::max(lim, 0);
+  }
+  delete[] h;
+  out->total_slabs = p.num_slabs;
+  out->used_slabs = handed - stacked - limbo;
+  out->limbo_slabs = limbo;
+  out->free_slabs = (uint64_t)p.num_slabs - out->used_slabs - limbo;
+  out->num_shards = p.num_shards;
+  out->tile_size = t->tile_size;
+  out->device_error = err[0];
+  out->device_error_count = err[1];
+  return MT_OK;
+}
+
+const char* mt_status_string(int s) {
+  switch (s) {
+    case MT_OK: return "ok";
+    case MT_ERR_OOM: return "slab pool exhausted";
+    case MT_ERR_LOCK_TIMEOUT: return "node lock timeout";
+    case MT_ERR_CORRUPT: return "corrupt index structure";
+    case MT_ERR_INVALID_ARG: return "invalid argument";
+    case MT_ERR_CUDA: return "CUDA error";
+    case MT_ERR_RETRY_LIMIT: return "retry limit reached";
+    case MT_ERR_KEY_TOO_LONG: return "key deeper than scan frame capacity";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

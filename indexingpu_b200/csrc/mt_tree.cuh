@@ -1,0 +1,814 @@
+// Device API of the B200 masstree: tile-cooperative find / insert / update /
+// erase / scan over a trie of B-link trees (one B-link tree per 4-byte key
+// slice).  These are the counterparts of the reference's
+// gpu_masstree::cooperative_{find,insert,update,erase,scan}
+// (include/gpu_masstree.hpp:194-248, 397-627, 629-749, 751-971, 250-395) and
+// keep their observable semantics:
+//   * find returns the FULL value length (0 = miss) and writes at most maxV
+//     value slices;
+//   * insert never overwrites unless update_if_exists; a key already present
+//     makes it return false;
+//   * update fails on a miss; erase returns whether the key was present;
+//   * scan visits keys in lexicographic u32-slice order (a key that is a prefix
+//     of another sorts first), both bounds inclusive.
+//
+// Concurrency: readers are lock-free and rely on a whole node being read by one
+// coalesced 128-byte access (the reference's assumption, README.md:168-172).
+// Writers lock a node through its meta word, publish the new node image with
+// release stores and release the lock with a separate release atomic.  Inserts
+// split full nodes top-down on the way to the border node (the proactive
+// B-link split of Awad et al., "Engineering a High-Performance GPU B-Tree",
+// PPoPP 2019, which the reference also uses, include/gpu_masstree.hpp:1020-1148).
+// Erase removes entries without merging nodes (the reference's merge_level 0):
+// results are identical, empty nodes stay linked.  Every spin and every retry
+// loop is bounded and records an error code instead of hanging.
+#pragma once
+#include "mt_suffix.cuh"
+
+namespace mtb {
+
+constexpr uint32_t kMaxHops = 1u << 16;     // node visits per operation
+constexpr uint32_t kLockSpins = 1u << 20;   // lock attempts before MT_ERR_LOCK_TIMEOUT
+constexpr uint32_t kMaxRestarts = 1u << 14;
+
+#ifndef MT_CONC_LOAD
+#define MT_CONC_LOAD ::mtb::ld_order::ACQUIRE
+#endif
+// Order of node loads in operations that run concurrently with writers.
+constexpr ld_order kConc = MT_CONC_LOAD;
+// Suffix chains are immutable after publication; they are read after the
+// owning entry was read with kConc, from L2.
+constexpr ld_order kConcSuffix = ld_order::RELAXED;
+
+enum op_result : int { R_ERR = -1, R_FAIL = 0, R_OK = 1 };
+
+struct tree_view {
+  pool_view pool;
+  uint32_t root;  // root slab of trie layer 0 (never moves)
+};
+
+// ---- locking -----------------------------------------------------------------
+
+template <int T>
+MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T>& nd) {
+  uint32_t* mw = p.addr(idx) + WORD_META;
+  for (uint32_t it = 0; it < kLockSpins; ++it) {
+    uint32_t old = 0;
+    if (t.leader()) old = atom_or_acquire(mw, META_LOCK);
+    old = t.shfl(old, 0);
+    if (!(old & META_LOCK)) {
+      t.sync();
+      nd.template load<ld_order::ACQUIRE>(t, p, idx);
+      return true;
+    }
+    if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
+    __nanosleep(32u << (it < 5u ? it : 5u));
+  }
+  if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT);
+  return false;
+}
+
+template <int T>
+MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
+  t.sync();
+  if (t.leader()) atom_and_release(p.addr(idx) + WORD_META, ~META_LOCK);
+  t.sync();
+}
+
+// Publish the node image; the stored meta keeps LOCK set.
+template <int T>
+MT_DEV void publish_locked(const tile<T>& t, const pool_view& p, node<T>& nd) {
+  nd.meta = (nd.meta | META_LOCK) + META_VERSION_ONE;
+  nd.encode_header(t);
+  nd.template store<st_order::RELEASE>(t, p);
+}
+
+// Publish the node image, then release its lock.
+template <int T>
+MT_DEV void publish_unlock(const tile<T>& t, const pool_view& p, node<T>& nd) {
+  publish_locked(t, p, nd);
+  unlock_node(t, p, nd.idx);
+  nd.meta &= ~META_LOCK;
+}
+
+// Write a node that no other tile can reach yet.
+template <int T>
+MT_DEV void publish_new(const tile<T>& t, const pool_view& p, node<T>& nd) {
+  nd.encode_header(t);
+  nd.template store<st_order::RELEASE>(t, p);
+}
+
+// Fresh layer root (an empty border node covering every slice).
+template <int T>
+MT_DEV void make_layer_root(const tile<T>& t, node<T>& nd, uint32_t idx) {
+  nd.clear_words();
+  nd.idx = idx;
+  nd.meta = META_BORDER | META_ROOT;
+  nd.ks = 0u;
+  nd.high = 0xFFFFFFFFu;
+  nd.sib = kInvalid;
+}
+
+// ---- descents ------------------------------------------------------------------
+
+// Lock-free descent of one layer to the border node covering `slice`.
+template <int T, ld_order O>
+MT_DEV bool descend(const tile<T>& t, const pool_view& p, uint32_t root, uint32_t slice,
+                    node<T>& nd, uint32_t& hops, uint32_t hop_limit = kMaxHops) {
+  uint32_t idx = root;
+  while (true) {
+    if (!p.valid(idx) || ++hops > hop_limit) {
+      if (t.leader()) record_error(p, ERR_CORRUPT);
+      return false;
+    }
+    nd.template load<O>(t, p, idx);
+    if (nd.must_move_right(slice)) { idx = nd.sib; continue; }
+    if (nd.is_border()) return true;
+    const int c = nd.child_pos(t, slice);
+    if (c < 0) {
+      if (t.leader()) record_error(p, ERR_CORRUPT);
+      return false;
+    }
+    idx = nd.val_at(t, (uint32_t)c);
+  }
+}
+
+// Lock the border node covering `slice`, starting from an unlocked image nd
+// obtained by a lock-free descent.  Moves right and re-descends as needed.
+template <int T>
+MT_DEV bool lock_border(const tile<T>& t, const pool_view& p, uint32_t slice, node<T>& nd, uint32_t& hops) {
+  uint32_t idx = nd.idx;
+  while (true) {
+    if (!p.valid(idx) || ++hops > kMaxHops) {
+      if (t.leader()) record_error(p, ERR_CORRUPT);
+      return false;
+    }
+    if (!lock_load(t, p, idx, nd)) return false;
+    if (nd.must_move_right(slice)) {
+      unlock_node(t, p, idx);
+      idx = nd.sib;
+      continue;
+    }
+    if (!nd.is_border()) {  // a layer root split after the lock-free descent
+      unlock_node(t, p, idx);
+      if (!descend<T, kConc>(t, p, idx, slice, nd, hops)) return false;
+      idx = nd.idx;
+      continue;
+    }
+    return true;
+  }
+}
+
+// Split position of a full node: never between the two entries of one slice.
+template <int T>
+MT_DEV uint32_t split_pos(const tile<T>& t, const node<T>& nd) {
+  uint32_t p = kMaxEntries / 2;
+  if (nd.is_border() && nd.key_at(t, p - 1) == nd.key_at(t, p)) ++p;
+  return p;
+}
+
+// Descent of one layer for an insert, splitting full nodes on the way.
+// Returns 0 with nd = the LOCKED, non-full border node covering `slice`;
+// 1 when the border node already holds a LINK for (slice, continues) (link set,
+// nothing locked); -1 on error.
+template <int T>
+MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& cache, uint32_t root,
+                         uint32_t slice, bool more, node<T>& nd, uint32_t& link, uint32_t& hops) {
+  uint32_t parent = kInvalid;
+  uint32_t idx = root;
+  uint32_t restarts = 0;
+  while (true) {
+    if (!p.valid(idx) || ++hops > kMaxHops) {
+      if (t.leader()) record_error(p, ERR_CORRUPT);
+      return -1;
+    }
+    nd.template load<kConc>(t, p, idx);
+    if (nd.must_move_right(slice)) { idx = nd.sib; continue; }
+    if (nd.is_border() && more) {
+      const int e = nd.match(t, slice, true);
+      if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { link = nd.val_at(t, (uint32_t)e); return 1; }
+    }
+    if (!nd.is_border() && !nd.full()) {
+      const int c = nd.child_pos(t, slice);
+      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+      parent = idx;
+      idx = nd.val_at(t, (uint32_t)c);
+      continue;
+    }
+    // Border node or full interior node: lock it.
+    if (!lock_load(t, p, idx, nd)) return -1;
+    if (nd.must_move_right(slice)) { unlock_node(t, p, idx); idx = nd.sib; continue; }
+    if (!nd.full()) {
+      if (nd.is_border()) return 0;
+      unlock_node(t, p, idx);
+      const int c = nd.child_pos(t, slice);
+      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+      parent = idx;
+      idx = nd.val_at(t, (uint32_t)c);
+      continue;
+    }
+    // nd is full and locked: split it.
+    const uint32_t sp = split_pos(t, nd);
+    const uint32_t left_high = nd.key_at(t, sp - 1);
+    const bool go_right = slice > left_high;
+    const bool border = nd.is_border();
+    node<T> rn;
+    if (nd.is_root()) {
+      // The layer root keeps its slab: its entries move to two new children.
+      const uint32_t L = cache.allocate(t, p);
+      const uint32_t R = (L != kInvalid) ? cache.allocate(t, p) : kInvalid;
+      if (R == kInvalid) {
+        if (L != kInvalid && t.leader()) retire_slab(p, L);
+        unlock_node(t, p, idx);
+        return -1;
+      }
+      node<T> ln;
+      rn.take_upper_from(t, nd, sp);
+      rn.idx = R;
+      rn.meta = (border ? META_BORDER : 0u) | (kMaxEntries - sp);
+      rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
+      rn.high = nd.high;
+      rn.sib = kInvalid;
+#pragma unroll
+      for (int k = 0; k < node<T>::W; ++k) ln.w[k] = nd.w[k];
+      ln.truncate(t, sp);
+      ln.idx = L;
+      ln.meta = (border ? META_BORDER : 0u) | META_SIB | sp;
+      ln.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
+      ln.high = left_high;
+      ln.sib = R;
+      // The child we continue into stays locked if it is a border node.
+      if (go_right && border) rn.meta |= META_LOCK;
+      if (!go_right && border) ln.meta |= META_LOCK;
+      publish_new(t, p, rn);
+      publish_new(t, p, ln);
+      const uint32_t old_high = nd.high;
+      nd.clear_words();
+      nd.set_word(t, 0, left_high);
+      nd.set_word(t, 1, L);
+      nd.set_word(t, 2, old_high);
+      nd.set_word(t, 3, R);
+      nd.meta = (nd.meta & ~(META_COUNT | META_BORDER)) | 2u;
+      nd.ks = 0u;
+      publish_unlock(t, p, nd);
+      parent = idx;
+      if (go_right) {
+        nd = rn;
+      } else {
+        nd = ln;
+      }
+    } else {
+      if (parent == kInvalid || ++restarts > kMaxRestarts) {
+        unlock_node(t, p, idx);
+        if (restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+        idx = root;
+        parent = kInvalid;
+        continue;
+      }
+      node<T> pn;
+      if (!lock_load(t, p, parent, pn)) { unlock_node(t, p, idx); return -1; }
+      const int j = pn.is_border() ? -1 : pn.child_slot_of(t, idx);
+      if (pn.full() || j < 0) {
+        // The parent changed under us: start the layer again.
+        unlock_node(t, p, parent);
+        unlock_node(t, p, idx);
+        if (++restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+        idx = root;
+        parent = kInvalid;
+        continue;
+      }
+      const uint32_t R = cache.allocate(t, p);
+      if (R == kInvalid) {
+        unlock_node(t, p, parent);
+        unlock_node(t, p, idx);
+        return -1;
+      }
+      rn.take_upper_from(t, nd, sp);
+      rn.idx = R;
+      rn.meta = (border ? META_BORDER : 0u) | (nd.meta & META_SIB) | (kMaxEntries - sp);
+      rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
+      rn.high = nd.high;
+      rn.sib = nd.sib;
+      if (go_right && border) rn.meta |= META_LOCK;
+      nd.truncate(t, sp);
+      nd.meta = (nd.meta & ~META_COUNT) | META_SIB | sp;
+      nd.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
+      nd.high = left_high;
+      nd.sib = R;
+      // Parent: (left_high -> idx) inserted at j; old entry j (-> idx) now -> R.
+      pn.insert_at(t, (uint32_t)j, left_high, idx, 0u);
+      pn.set_entry(t, (uint32_t)j + 1u, R, 0u);
+      // Write order: right, left, parent.
+      publish_new(t, p, rn);
+      publish_locked(t, p, nd);
+      publish_unlock(t, p, pn);
+      if (go_right) {
+        unlock_node(t, p, idx);
+        nd = rn;
+      }
+      parent = pn.idx;  // both halves hang under pn
+    }
+    // nd is now the non-full half covering slice; locked iff border.
+    if (nd.is_border()) {
+      nd.meta |= META_LOCK;
+      return 0;
+    }
+    if (nd.locked()) unlock_node(t, p, nd.idx);
+    const int c = nd.child_pos(t, slice);
+    if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+    parent = nd.idx;
+    idx = nd.val_at(t, (uint32_t)c);
+  }
+}
+
+// ---- find ------------------------------------------------------------------------
+
+template <int T, bool CONCURRENT>
+MT_DEV uint32_t coop_find(const tile<T>& t, const tree_view& tv, const uint32_t* key, uint32_t klen,
+                          uint32_t* out, uint32_t maxV) {
+  constexpr ld_order O = CONCURRENT ? kConc : ld_order::NC;
+  constexpr ld_order OS = CONCURRENT ? kConcSuffix : ld_order::NC;
+  const pool_view& p = tv.pool;
+  uint32_t root = tv.root, hops = 0;
+  node<T> nd;
+  for (uint32_t layer = 0; layer < klen; ++layer) {
+    const uint32_t slice = key[layer];
+    const bool more = layer + 1u < klen;
+    if (!descend<T, O>(t, p, root, slice, nd, hops)) return 0u;
+    const int e = nd.match(t, slice, more);
+    if (e < 0) return 0u;
+    const uint32_t st = ks_get(nd.ks, (uint32_t)e);
+    const uint32_t v = nd.val_at(t, (uint32_t)e);
+    if (st == KS_LINK) { root = v; continue; }
+    if (st == KS_VALUE) {
+      if (maxV > 0u && out != nullptr && t.leader()) out[0] = v;
+      return 1u;
+    }
+    if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT); return 0u; }
+    suffix_head<T> h;
+    h.template load<OS>(t, p, v);
+    if (st == KS_SUFFIX) {
+      const uint32_t lk = klen - layer - 1u;
+      if (h.klen != lk) return 0u;
+      if (suffix_compare<T, OS>(t, p, h, key + layer + 1u, lk).sign != 0) return 0u;
+    }
+    return suffix_get_value<T, OS>(t, p, h, out, maxV);
+  }
+  return 0u;
+}
+
+// ---- helpers shared by insert and update -----------------------------------------
+
+// New representation of a value: inline for length 1, else a LONGVAL chain.
+template <int T>
+MT_DEV bool make_value(const tile<T>& t, const pool_view& p, slab_cache<T>& cache,
+                       const uint32_t* val, uint32_t vlen, uint32_t& nv, uint32_t& ns) {
+  if (vlen == 1u) {
+    nv = val[0];
+    ns = KS_VALUE;
+    return true;
+  }
+  slice_src k, v;
+  v.ptr = val;
+  v.len = vlen;
+  nv = suffix_create<T, kConcSuffix>(t, p, cache, k, v);
+  ns = KS_LONGVAL;
+  return nv != kInvalid;
+}
+
+// Replace the value of entry e (VALUE/LONGVAL) of the locked border node.
+template <int T>
+MT_DEV int replace_value(const tile<T>& t, const pool_view& p, slab_cache<T>& cache, node<T>& nd,
+                         uint32_t e, uint32_t old_state, uint32_t old_val, const uint32_t* val, uint32_t vlen) {
+  uint32_t nv, ns;
+  if (!make_value(t, p, cache, val, vlen, nv, ns)) {
+    unlock_node(t, p, nd.idx);
+    return R_ERR;
+  }
+  nd.set_entry(t, e, nv, ns);
+  publish_unlock(t, p, nd);
+  if (old_state == KS_LONGVAL) suffix_retire<T, kConcSuffix>(t, p, old_val);
+  return R_OK;
+}
+
+// Replace a SUFFIX entry whose key rest equals K with a chain holding K + val.
+template <int T>
+MT_DEV int replace_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& cache, node<T>& nd,
+                          uint32_t e, uint32_t old_chain, const uint32_t* K, uint32_t lk,
+                          const uint32_t* val, uint32_t vlen) {
+  slice_src ks, vs;
+  ks.ptr = K;
+  ks.len = lk;
+  vs.ptr = val;
+  vs.len = vlen;
+  const uint32_t nv = suffix_create<T, kConcSuffix>(t, p, cache, ks, vs);
+  if (nv == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+  nd.set_entry(t, e, nv, KS_SUFFIX);
+  publish_unlock(t, p, nd);
+  suffix_retire<T, kConcSuffix>(t, p, old_chain);
+  return R_OK;
+}
+
+// Entry payload for a key tail: (slice at position m of K, state, value).
+// K[0..lk) is the key rest after the border slice; `m` indexes it.
+template <int T>
+MT_DEV bool make_tail_entry(const tile<T>& t, const pool_view& p, slab_cache<T>& cache,
+                            const slice_src& K, uint32_t lk, uint32_t m, const slice_src& V,
+                            uint32_t& slice, uint32_t& state, uint32_t& value) {
+  const bool more = m + 1u < lk;
+  if (K.ptr) slice = K.ptr[m];
+  else slice = chain_slice<kConcSuffix>(p, K.chain, K.offset + m);
+  if (more) {
+    slice_src rest = K;
+    if (rest.ptr) rest.ptr += m + 1u;
+    else rest.offset += m + 1u;
+    rest.len = lk - m - 1u;
+    value = suffix_create<T, kConcSuffix>(t, p, cache, rest, V);
+    state = KS_SUFFIX;
+    return value != kInvalid;
+  }
+  if (V.len == 1u) {
+    value = V.ptr ? V.ptr[0] : chain_slice<kConcSuffix>(p, V.chain, V.offset);
+    state = KS_VALUE;
+    return true;
+  }
+  slice_src none;
+  value = suffix_create<T, kConcSuffix>(t, p, cache, none, V);
+  state = KS_LONGVAL;
+  return value != kInvalid;
+}
+
+// Two keys share a SUFFIX entry's slice but differ later: replace the entry by a
+// LINK to a chain of single-entry layers for the common slices, ending in a layer
+// with one entry per key (the reference's singleton/doubleton conversion,
+// include/gpu_masstree.hpp:533-577).
+template <int T>
+MT_DEV int split_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& cache, node<T>& nd,
+                        uint32_t e, const suffix_head<T>& h, uint32_t first_diff,
+                        const uint32_t* K, uint32_t lk, const uint32_t* val, uint32_t vlen) {
+  const uint32_t ls = h.klen;
+  const uint32_t m = min(first_diff, min(ls, lk) - 1u);
+  // Old key tail and value live in the old chain.
+  slice_src oldK, oldV, newK, newV;
+  oldK.chain = h.idx; oldK.offset = 0; oldK.len = ls;
+  oldV.chain = h.idx; oldV.offset = ls; oldV.len = h.vlen;
+  newK.ptr = K; newK.len = lk;
+  newV.ptr = val; newV.len = vlen;
+  uint32_t so, sto, vo, sn, stn, vn;
+  if (!make_tail_entry(t, p, cache, oldK, ls, m, oldV, so, sto, vo)) { unlock_node(t, p, nd.idx); return R_ERR; }
+  if (!make_tail_entry(t, p, cache, newK, lk, m, newV, sn, stn, vn)) { unlock_node(t, p, nd.idx); return R_ERR; }
+  // Doubleton layer root.
+  const uint32_t dslab = cache.allocate(t, p);
+  if (dslab == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+  node<T> ln;
+  make_layer_root(t, ln, dslab);
+  if (pos_less(so, ks_more(sto), sn, ks_more(stn))) {
+    ln.insert_at(t, 0, so, vo, sto);
+    ln.insert_at(t, 1, sn, vn, stn);
+  } else {
+    ln.insert_at(t, 0, sn, vn, stn);
+    ln.insert_at(t, 1, so, vo, sto);
+  }
+  publish_new(t, p, ln);
+  // Singleton layers for the common slices K[m-1] .. K[0], built bottom-up.
+  uint32_t below = dslab;
+  for (int i = (int)m - 1; i >= 0; --i) {
+    const uint32_t s = cache.allocate(t, p);
+    if (s == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+    make_layer_root(t, ln, s);
+    ln.insert_at(t, 0, K[i], below, KS_LINK);
+    publish_new(t, p, ln);
+    below = s;
+  }
+  nd.set_entry(t, e, below, KS_LINK);
+  publish_unlock(t, p, nd);
+  suffix_retire<T, kConcSuffix>(t, p, h.idx);
+  return R_OK;
+}
+
+// ---- insert ------------------------------------------------------------------------
+
+template <int T, bool UPSERT>
+MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const uint32_t* key,
+                       uint32_t klen, const uint32_t* val, uint32_t vlen) {
+  const pool_view& p = tv.pool;
+  if (klen == 0u || vlen > kMaxLen16 || klen > kMaxLen16) {
+    if (t.leader()) record_error(p, ERR_INVALID_ARG);
+    return R_ERR;
+  }
+  uint32_t root = tv.root, hops = 0;
+  node<T> nd;
+  for (uint32_t layer = 0; layer < klen;) {
+    const uint32_t slice = key[layer];
+    const bool more = layer + 1u < klen;
+    uint32_t link = kInvalid;
+    const int r = descend_split(t, p, cache, root, slice, more, nd, link, hops);
+    if (r < 0) return R_ERR;
+    if (r == 1) { root = link; ++layer; continue; }
+    const int e = nd.match(t, slice, more);
+    if (e >= 0) {
+      const uint32_t st = ks_get(nd.ks, (uint32_t)e);
+      const uint32_t v = nd.val_at(t, (uint32_t)e);
+      if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
+      if (st == KS_VALUE || st == KS_LONGVAL) {
+        if (!UPSERT) { unlock_node(t, p, nd.idx); return R_FAIL; }
+        return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
+      }
+      // SUFFIX entry: same key, or a different key sharing this slice.
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+      suffix_head<T> h;
+      h.template load<kConcSuffix>(t, p, v);
+      const uint32_t lk = klen - layer - 1u;
+      const cmp_result c = suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk);
+      if (c.sign == 0) {
+        if (!UPSERT) { unlock_node(t, p, nd.idx); return R_FAIL; }
+        return replace_suffix(t, p, cache, nd, (uint32_t)e, v, key + layer + 1u, lk, val, vlen);
+      }
+      return split_suffix(t, p, cache, nd, (uint32_t)e, h, c.first_diff, key + layer + 1u, lk, val, vlen);
+    }
+    // Absent: add one entry.
+    uint32_t nv, ns;
+    if (more) {
+      slice_src ks, vs;
+      ks.ptr = key + layer + 1u;
+      ks.len = klen - layer - 1u;
+      vs.ptr = val;
+      vs.len = vlen;
+      nv = suffix_create<T, kConcSuffix>(t, p, cache, ks, vs);
+      ns = KS_SUFFIX;
+      if (nv == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+    } else if (!make_value(t, p, cache, val, vlen, nv, ns)) {
+      unlock_node(t, p, nd.idx);
+      return R_ERR;
+    }
+    nd.insert_at(t, nd.lower_pos(t, slice, more), slice, nv, ns);
+    publish_unlock(t, p, nd);
+    return R_OK;
+  }
+  return R_ERR;
+}
+
+// ---- update -------------------------------------------------------------------------
+
+template <int T>
+MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const uint32_t* key,
+                       uint32_t klen, const uint32_t* val, uint32_t vlen) {
+  const pool_view& p = tv.pool;
+  if (klen == 0u || vlen > kMaxLen16) {
+    if (t.leader()) record_error(p, ERR_INVALID_ARG);
+    return R_ERR;
+  }
+  uint32_t root = tv.root, hops = 0;
+  node<T> nd;
+  for (uint32_t layer = 0; layer < klen;) {
+    const uint32_t slice = key[layer];
+    const bool more = layer + 1u < klen;
+    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return R_ERR;
+    if (more) {
+      const int e = nd.match(t, slice, true);
+      if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
+    }
+    if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
+    const int e = nd.match(t, slice, more);
+    if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
+    const uint32_t st = ks_get(nd.ks, (uint32_t)e);
+    const uint32_t v = nd.val_at(t, (uint32_t)e);
+    if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
+    if (st == KS_VALUE || st == KS_LONGVAL) return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
+    if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+    suffix_head<T> h;
+    h.template load<kConcSuffix>(t, p, v);
+    const uint32_t lk = klen - layer - 1u;
+    if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
+      unlock_node(t, p, nd.idx);
+      return R_FAIL;
+    }
+    return replace_suffix(t, p, cache, nd, (uint32_t)e, v, key + layer + 1u, lk, val, vlen);
+  }
+  return R_FAIL;
+}
+
+// ---- erase --------------------------------------------------------------------------
+
+template <int T>
+MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key, uint32_t klen) {
+  const pool_view& p = tv.pool;
+  if (klen == 0u) return R_FAIL;
+  uint32_t root = tv.root, hops = 0;
+  node<T> nd;
+  for (uint32_t layer = 0; layer < klen;) {
+    const uint32_t slice = key[layer];
+    const bool more = layer + 1u < klen;
+    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return R_ERR;
+    if (more) {
+      const int e = nd.match(t, slice, true);
+      if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
+    }
+    if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
+    const int e = nd.match(t, slice, more);
+    if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
+    const uint32_t st = ks_get(nd.ks, (uint32_t)e);
+    const uint32_t v = nd.val_at(t, (uint32_t)e);
+    if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
+    if (st == KS_SUFFIX) {
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+      suffix_head<T> h;
+      h.template load<kConcSuffix>(t, p, v);
+      const uint32_t lk = klen - layer - 1u;
+      if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
+        unlock_node(t, p, nd.idx);
+        return R_FAIL;
+      }
+    }
+    nd.remove_at(t, (uint32_t)e);
+    publish_unlock(t, p, nd);
+    if (st != KS_VALUE) suffix_retire<T, kConcSuffix>(t, p, v);
+    return R_OK;
+  }
+  return R_FAIL;
+}
+
+// ---- scan ----------------------------------------------------------------------------
+
+// Per-layer scan frame kept in global scratch: border node holding the LINK we
+// descended through, the LINK's slice, and whether the layer was on the upper
+// bound's path.
+struct scan_frame {
+  uint32_t node;
+  uint32_t slice;
+  uint32_t upper_tight;
+  uint32_t pad;
+};
+
+struct scan_out {
+  uint32_t* values;
+  uint32_t* value_lengths;
+  uint32_t maxV;
+  uint32_t* keys;
+  uint32_t* key_lengths;
+  uint32_t maxK;
+};
+
+// Emit one result: key = frames[0..layer) slices ++ slice ++ suffix rest.
+template <int T, ld_order OS>
+MT_DEV void scan_emit(const tile<T>& t, const pool_view& p, const scan_frame* frames, uint32_t layer,
+                      uint32_t slice, uint32_t state, uint32_t v, const suffix_head<T>* h,
+                      const scan_out& o, uint32_t c) {
+  uint32_t rest = 0, vlen = 1;
+  if (state != KS_VALUE) { rest = h->klen; vlen = h->vlen; }
+  const uint32_t klen = layer + 1u + rest;
+  if (o.keys) {
+    uint32_t* row = o.keys + (size_t)c * o.maxK;
+    for (uint32_t i = t.rank; i < layer && i < o.maxK; i += T) row[i] = frames[i].slice;
+    if (t.leader() && layer < o.maxK) row[layer] = slice;
+    if (rest) {
+      // Key rest: data slices [0, rest) of the chain.
+      constexpr int W = 32 / T;
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const uint32_t g = t.rank * W + q;
+        if (g < kSufData && g < rest && layer + 1u + g < o.maxK) row[layer + 1u + g] = h->w[q];
+      }
+      for (uint32_t i = kSufData + t.rank; i < rest && layer + 1u + i < o.maxK; i += T)
+        row[layer + 1u + i] = chain_slice<OS>(p, h->idx, i);
+    }
+  }
+  if (o.key_lengths && t.leader()) o.key_lengths[c] = klen;
+  if (o.value_lengths && t.leader()) o.value_lengths[c] = vlen;
+  if (o.values && o.maxV > 0u) {
+    uint32_t* vrow = o.values + (size_t)c * o.maxV;
+    if (state == KS_VALUE) {
+      if (t.leader()) vrow[0] = v;
+    } else {
+      suffix_get_value<T, OS>(t, p, *h, vrow, o.maxV);
+    }
+  }
+}
+
+// Ordered scan from `lower` (inclusive) for at most max_count keys, stopping
+// after `upper` (inclusive) when use_upper.  frames: scratch of frame_cap frames
+// for this tile.  Returns the number of keys written.
+template <int T, bool CONCURRENT>
+MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t* lower, uint32_t llen,
+                          bool use_upper, const uint32_t* upper, uint32_t ulen, uint32_t max_count,
+                          const scan_out& o, scan_frame* frames, uint32_t frame_cap) {
+  constexpr ld_order O = CONCURRENT ? kConc : ld_order::NC;
+  constexpr ld_order OS = CONCURRENT ? kConcSuffix : ld_order::NC;
+  const pool_view& p = tv.pool;
+  if (max_count == 0u) return 0u;
+  if (use_upper && ulen == 0u) return 0u;
+  uint32_t count = 0, hops = 0, layer = 0;
+  const uint32_t hop_limit = kMaxHops + 8u * max_count;
+  bool ltight = llen > 0u;   // still on the lower bound's path
+  bool utight = use_upper;   // still on the upper bound's path
+  node<T> nd;
+  uint32_t start;
+  // Enter layer 0.
+  {
+    const uint32_t s0 = ltight ? lower[0] : 0u;
+    if (!descend<T, O>(t, p, tv.root, s0, nd, hops, hop_limit)) return 0u;
+    start = ltight ? nd.lower_pos(t, s0, llen > 1u) : 0u;
+  }
+  while (true) {
+    // Walk entries [start, count) of the border node nd at `layer`.
+    bool descended = false;
+    const uint32_t n = nd.count();
+    for (uint32_t e = start; e < n; ++e) {
+      const uint32_t s = nd.key_at(t, e);
+      const uint32_t st = ks_get(nd.ks, e);
+      const uint32_t v = nd.val_at(t, e);
+      const bool more = ks_more(st);
+      bool child_ltight = false;
+      bool child_utight = false;
+      suffix_head<T> h;
+      const bool has_chain = st == KS_SUFFIX || st == KS_LONGVAL;
+      if (has_chain) {
+        if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+        h.template load<OS>(t, p, v);
+      }
+      if (ltight) {
+        const uint32_t ls = lower[layer];
+        const bool lm = layer + 1u < llen;
+        if (pos_less(s, more, ls, lm)) continue;
+        if (s == ls && more == lm) {
+          if (st == KS_SUFFIX) {
+            if (suffix_compare<T, OS>(t, p, h, lower + layer + 1u, llen - layer - 1u).sign < 0) continue;
+          } else if (st == KS_LINK) {
+            child_ltight = true;
+          }
+        }
+        ltight = false;
+      }
+      if (utight) {
+        const uint32_t us = upper[layer];
+        const bool um = layer + 1u < ulen;
+        if (pos_less(us, um, s, more)) return count;  // entry beyond upper
+        if (s == us && more == um) {
+          if (st == KS_SUFFIX) {
+            if (suffix_compare<T, OS>(t, p, h, upper + layer + 1u, ulen - layer - 1u).sign > 0) return count;
+          } else if (st == KS_LINK) {
+            child_utight = true;
+          }
+        }
+      }
+      if (st == KS_LINK) {
+        if (layer + 1u >= frame_cap) { if (t.leader()) record_error(p, ERR_KEY_TOO_LONG); return count; }
+        if (t.leader()) {
+          scan_frame f;
+          f.node = nd.idx;
+          f.slice = s;
+          f.upper_tight = utight ? 1u : 0u;
+          f.pad = 0u;
+          frames[layer] = f;
+        }
+        t.sync();
+        ++layer;
+        ltight = child_ltight;
+        utight = child_utight;
+        const uint32_t s0 = ltight ? lower[layer] : 0u;
+        if (!descend<T, O>(t, p, v, s0, nd, hops, hop_limit)) return count;
+        start = ltight ? nd.lower_pos(t, s0, layer + 1u < llen) : 0u;
+        descended = true;
+        break;
+      }
+      scan_emit<T, OS>(t, p, frames, layer, s, st, v, has_chain ? &h : nullptr, o, count);
+      ++count;
+      if (count >= max_count) return count;
+      if (utight && s == upper[layer] && more == (layer + 1u < ulen)) return count;  // emitted upper itself
+    }
+    if (descended) continue;
+    ltight = false;
+    // Next border node of this layer.
+    if (nd.has_sib()) {
+      if (utight && nd.high >= upper[layer]) return count;
+      const uint32_t sib = nd.sib;
+      if (!p.valid(sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+      nd.template load<O>(t, p, sib);
+      start = 0;
+      continue;
+    }
+    // End of this layer: resume the parent layer after the LINK slice.
+    if (layer == 0u) return count;
+    t.sync();
+    --layer;
+    const scan_frame f = frames[layer];
+    utight = f.upper_tight != 0u;
+    if (utight && f.slice == upper[layer]) return count;  // the LINK was upper's own path
+    if (f.slice == 0xFFFFFFFFu) {
+      // Nothing can follow slice 0xFFFFFFFF in this layer.
+      nd.meta = 0u;  // empty image: fall through to sibling/pop handling
+      nd.idx = f.node;
+      start = 0;
+      continue;
+    }
+    if (!p.valid(f.node)) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+    nd.template load<O>(t, p, f.node);
+    while (nd.must_move_right(f.slice)) {
+      if (!p.valid(nd.sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+      nd.template load<O>(t, p, nd.sib);
+    }
+    start = __popc(nd.entry_mask(t, [&](uint32_t k, uint32_t) { return k <= f.slice; }));
+  }
+}
+
+}  // namespace mtb

@@ -1,0 +1,157 @@
+"""Python mirror of IndexinGPU's gpu_masstree host API over libmt_b200.so.
+
+Method names, argument order and meaning follow the reference's
+GpuMasstree::gpu_masstree (include/gpu_masstree.hpp:84-191):
+
+    find(keys, max_key_length, key_lengths, values, max_value_length,
+         value_lengths, num_keys, stream=0)
+    insert / update(keys, max_key_length, key_lengths, values,
+         max_value_length, value_lengths, num_keys, stream=0)
+    erase(keys, max_key_length, key_lengths, num_keys, stream=0)
+    scan(lower_keys, lower_key_lengths, max_key_length, max_count_per_query,
+         num_queries, upper_keys=None, upper_key_lengths=None, counts=None,
+         values=None, max_value_length=1, value_lengths=None, out_keys=None,
+         out_key_lengths=None, stream=0)
+    mixed_batch(request_types, keys, max_key_length, key_lengths, values,
+         max_value_length, value_lengths, results, num_requests, stream=0)
+
+The reference's compile-time switches become keyword arguments
+(concurrent=, update_if_exists=, use_upper_key=).  Buffers are torch tensors in
+device memory or pinned host memory (or raw integer addresses); None means the
+reference's nullptr.  Calls are asynchronous; sync() waits and raises on a
+device-side error.
+"""
+import ctypes
+
+from . import _lib
+
+REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
+FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY = 1, 2, 4
+STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
+          5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG"}
+
+
+class MasstreeError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__(f"{what}: {STATUS.get(code, code)}")
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x or None
+    return x.data_ptr()
+
+
+def _stream(s):
+    if s is None or s == 0:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream  # torch.cuda.Stream
+
+
+class GpuMasstree:
+    """Ordered GPU index over variable-length u32-slice keys and values."""
+
+    def __init__(self, pool_ratio=0.9, tile_size=8, pool_bytes=None):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        if pool_bytes is not None:
+            rc = self._lib.mt_create_bytes(ctypes.byref(h), int(pool_bytes), tile_size)
+        else:
+            rc = self._lib.mt_create(ctypes.byref(h), float(pool_ratio), tile_size)
+        self._check(rc, "mt_create")
+        self._h = h
+
+    # -- lifetime ---------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _check(rc, what):
+        if rc != 0:
+            raise MasstreeError(rc, what)
+
+    # -- configuration ------------------------------------------------------------
+    def set_tile_size(self, tile_size):
+        self._check(self._lib.mt_set_tile_size(self._h, tile_size), "mt_set_tile_size")
+
+    def set_blocks_per_sm(self, blocks_per_sm):
+        self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
+
+    # -- host API (reference gpu_masstree.hpp:86-191) ----------------------------
+    def find(self, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, num_keys,
+             stream=0, concurrent=False):
+        rc = self._lib.mt_find(self._h, _ptr(keys), max_key_length, _ptr(key_lengths), _ptr(values),
+                               max_value_length, _ptr(value_lengths), num_keys,
+                               FLAG_CONCURRENT if concurrent else 0, _stream(stream))
+        self._check(rc, "mt_find")
+
+    def insert(self, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, num_keys,
+               stream=0, update_if_exists=False, results=None):
+        rc = self._lib.mt_insert(self._h, _ptr(keys), max_key_length, _ptr(key_lengths), _ptr(values),
+                                 max_value_length, _ptr(value_lengths), num_keys, _ptr(results),
+                                 FLAG_UPDATE_IF_EXISTS if update_if_exists else 0, _stream(stream))
+        self._check(rc, "mt_insert")
+
+    def update(self, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, num_keys,
+               stream=0, results=None):
+        rc = self._lib.mt_update(self._h, _ptr(keys), max_key_length, _ptr(key_lengths), _ptr(values),
+                                 max_value_length, _ptr(value_lengths), num_keys, _ptr(results), 0,
+                                 _stream(stream))
+        self._check(rc, "mt_update")
+
+    def erase(self, keys, max_key_length, key_lengths, num_keys, stream=0, results=None):
+        rc = self._lib.mt_erase(self._h, _ptr(keys), max_key_length, _ptr(key_lengths), num_keys, _ptr(results),
+                                0, _stream(stream))
+        self._check(rc, "mt_erase")
+
+    def scan(self, lower_keys, lower_key_lengths, max_key_length, max_count_per_query, num_queries,
+             upper_keys=None, upper_key_lengths=None, counts=None, values=None, max_value_length=1,
+             value_lengths=None, out_keys=None, out_key_lengths=None, stream=0, use_upper_key=None,
+             concurrent=False):
+        if use_upper_key is None:
+            use_upper_key = upper_keys is not None
+        flags = (FLAG_USE_UPPER_KEY if use_upper_key else 0) | (FLAG_CONCURRENT if concurrent else 0)
+        rc = self._lib.mt_scan(self._h, _ptr(lower_keys), _ptr(lower_key_lengths), max_key_length,
+                               max_count_per_query, num_queries, _ptr(upper_keys), _ptr(upper_key_lengths),
+                               _ptr(counts), _ptr(values), max_value_length, _ptr(value_lengths), _ptr(out_keys),
+                               _ptr(out_key_lengths), flags, _stream(stream))
+        self._check(rc, "mt_scan")
+
+    def mixed_batch(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
+                    value_lengths, results, num_requests, stream=0):
+        rc = self._lib.mt_mixed_batch(self._h, _ptr(request_types), _ptr(keys), max_key_length, _ptr(key_lengths),
+                                      _ptr(values), max_value_length, _ptr(value_lengths), _ptr(results),
+                                      num_requests, 0, _stream(stream))
+        self._check(rc, "mt_mixed_batch")
+
+    # -- status ---------------------------------------------------------------------
+    def sync(self, stream=0):
+        """Wait for the stream; raise MasstreeError if a device error was recorded."""
+        self._check(self._lib.mt_sync(self._h, _stream(stream)), "device")
+
+    def reclaim(self, stream=0):
+        self._check(self._lib.mt_reclaim(self._h, _stream(stream)), "mt_reclaim")
+
+    def stats(self):
+        s = _lib.MtStats()
+        self._check(self._lib.mt_stats(self._h, ctypes.byref(s)), "mt_stats")
+        return {f: getattr(s, f) for f, _ in _lib.MtStats._fields_}

@@ -1,0 +1,261 @@
+"""Parity of the CUDA library with the CPU oracle and with the reference's own
+gpu_masstree on seeded workloads shaped like the benchmark configurations, at
+sizes the oracle finishes in seconds.  Integer results must match bit-for-bit.
+"""
+import numpy as np
+import pytest
+
+from indexes import GpuIndex, OracleIndex, RefIndex
+from indexingpu_b200 import workload as wl
+from oracle.pyoracle import RefMasstree
+from scenarios import assert_found
+
+pytestmark = pytest.mark.gpu
+TILES = [4, 8, 16, 32]
+
+
+@pytest.fixture(params=TILES)
+def tile(request):
+    return request.param
+
+
+def dump_via_scan(idx, maxK, maxV, n_expected):
+    """Every key in order, by one scan from the smallest possible key."""
+    lower = np.zeros((1, maxK), np.uint32)
+    counts, vals, vlens, okeys, oklens = idx.scan(lower, np.ones(1, np.uint32), n_expected + 8, maxV=maxV)
+    c = int(counts[0])
+    return okeys[0, :c], oklens[0, :c], vals[0, :c], vlens[0, :c]
+
+
+def assert_same_state(a, b, what):
+    ka, la, va, vla = a
+    kb, lb, vb, vlb = b
+    assert len(la) == len(lb), f"{what}: {len(la)} vs {len(lb)} keys"
+    np.testing.assert_array_equal(la, lb, err_msg=f"{what}: key lengths")
+    np.testing.assert_array_equal(vla, vlb, err_msg=f"{what}: value lengths")
+    for i in range(len(la)):
+        L = la[i]
+        assert np.array_equal(ka[i, :L], kb[i, :L]), f"{what}: key {i}"
+        c = min(int(vla[i]), va.shape[1])
+        assert np.array_equal(va[i, :c], vb[i, :c]), f"{what}: value {i}"
+
+
+def test_c1_insert_find(tile):
+    w = wl.c1(n_keys=20000, n_finds=20000)
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        rg = g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        ro = o.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        np.testing.assert_array_equal(rg, ro)
+        assert rg.all()
+        for conc in (False, True):
+            vg, lg = g.find(w["find_keys"], w["find_lens"], 2, concurrent=conc)
+            vo, lo = o.find(w["find_keys"], w["find_lens"], 2)
+            assert_found(vg, lg, vo, lo, f"c1 find concurrent={conc}")
+            assert (lg > 0).sum() == w["find_hit"].sum()
+    finally:
+        g.close()
+
+
+def test_find_value_truncation_and_null_lengths(tile):
+    # Stored values longer than max_value_length: the full length is returned
+    # and max_value_length slices are written.
+    keys = np.arange(1, 301, dtype=np.uint32).reshape(100, 3)
+    lens = np.full(100, 3, np.uint32)
+    vals = np.tile(np.arange(7, dtype=np.uint32), (100, 1)) + keys[:, :1]
+    vlens = np.full(100, 7, np.uint32)
+    g = GpuIndex(tile)
+    try:
+        g.insert(keys, lens, vals, vlens)
+        v, l = g.find(keys, None, 3)  # NULL key lengths -> every key has max length 3
+        assert (l == 7).all()
+        np.testing.assert_array_equal(v, vals[:, :3])
+    finally:
+        g.close()
+
+
+def test_upsert_and_results(tile):
+    w = wl.c1(n_keys=5000, n_finds=10)
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        o.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        v2 = w["vals"] ^ np.uint32(0x5A5A5A5A)
+        # Mixed 1-slice and 2-slice new values: VALUE <-> LONGVAL transitions.
+        vl2 = (1 + (np.arange(len(v2)) % 2)).astype(np.uint32)
+        np.testing.assert_array_equal(g.insert(w["keys"], w["lens"], v2, vl2, upsert=True),
+                                      o.insert(w["keys"], w["lens"], v2, vl2, upsert=True))
+        vg, lg = g.find(w["keys"], w["lens"], 2)
+        vo, lo = o.find(w["keys"], w["lens"], 2)
+        assert_found(vg, lg, vo, lo, "upsert")
+        # Plain insert of existing keys fails everywhere.
+        assert not g.insert(w["keys"], w["lens"], v2, vl2).any()
+    finally:
+        g.close()
+
+
+def _touch_once_batches(c2, n_batches, n):
+    """Mixed batches in which every key appears at most once (per-request
+    results are order independent)."""
+    out = []
+    for b in range(n_batches):
+        bt = c2.batch(b, n)
+        _, first = np.unique(bt["ids"], return_index=True)
+        keep = np.sort(first)
+        out.append({k: v[keep] for k, v in bt.items()})
+    return out
+
+
+@pytest.mark.parametrize("n_preload", [3000, 40000])
+def test_c2_mixed_touch_once(tile, n_preload):
+    c2 = wl.C2(n_preload=n_preload, n_prefixes=64)
+    keys, lens, vals, vlens = c2.keys(np.arange(n_preload))
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(keys, lens, vals, vlens)
+        o.insert(keys, lens, vals, vlens)
+        for bt in _touch_once_batches(c2, 4, 8000):
+            gv, gl, gr = g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            ov, ol, orr = o.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            notfind = bt["types"] != wl.REQ_FIND
+            np.testing.assert_array_equal(gr[notfind], orr[notfind], err_msg="mixed results")
+            f = ~notfind
+            assert_found(gv[f], gl[f], ov[f], ol[f], "mixed finds")
+        assert_same_state(dump_via_scan(g, 16, 8, o.o.size()), o.dump(16, 8), "final state")
+    finally:
+        g.close()
+
+
+def test_c2_mixed_zipf_final_state(tile):
+    """Zipf batches with repeated keys: final key set and values are
+    deterministic (fresh inserts, key-determined update values, erase wins)."""
+    c2 = wl.C2(n_preload=20000, n_prefixes=64)
+    keys, lens, vals, vlens = c2.keys(np.arange(20000))
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(keys, lens, vals, vlens)
+        o.insert(keys, lens, vals, vlens)
+        for b in range(3):
+            bt = c2.batch(b, 20000)
+            # Deterministic final state: updates of a key that the batch also
+            # erases are dropped from both sides' final comparison by erasing
+            # last; run updates only on keys not erased in this batch.
+            er = set(bt["ids"][bt["types"] == wl.REQ_ERASE].tolist())
+            keep = np.array([not (t == wl.REQ_UPDATE and i in er) for t, i in zip(bt["types"], bt["ids"])])
+            bt = {k: v[keep] for k, v in bt.items()}
+            g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            o.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+        assert_same_state(dump_via_scan(g, 16, 8, o.o.size()), o.dump(16, 8), "final state")
+    finally:
+        g.close()
+
+
+def test_c3_scan(tile):
+    w = wl.c3(50000, 3000)
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        o.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        rg = g.scan(w["lower"], w["lower_lens"], 100, maxV=1)
+        ro = o.scan(w["lower"], w["lower_lens"], 100, maxV=1)
+        for a, b, name in zip(rg, ro, ["counts", "values", "value_lengths", "keys", "key_lengths"]):
+            np.testing.assert_array_equal(a, b, err_msg=f"scan {name}")
+    finally:
+        g.close()
+
+
+def test_scan_with_upper_varlen(tile):
+    c2 = wl.C2(n_preload=30000, n_prefixes=16)
+    keys, lens, vals, vlens = c2.keys(np.arange(30000))
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(keys, lens, vals, vlens)
+        o.insert(keys, lens, vals, vlens)
+        rng = np.random.default_rng(5)
+        a = rng.integers(0, 30000, 2000)
+        b = rng.integers(0, 30000, 2000)
+        lo_k, lo_l = keys[a].copy(), lens[a].copy()
+        up_k, up_l = keys[b].copy(), lens[b].copy()
+        # Some bounds are shortened prefixes of stored keys (absent keys).
+        cut = rng.random(2000) < 0.3
+        lo_l = np.where(cut, np.maximum(1, lo_l - 1), lo_l)
+        for mc in (7, 50):
+            rg = g.scan(lo_k, lo_l, mc, up_k, up_l, maxV=8)
+            ro = o.scan(lo_k, lo_l, mc, up_k, up_l, maxV=8)
+            np.testing.assert_array_equal(rg[0], ro[0], err_msg="counts")
+            for q in range(2000):
+                c = int(ro[0][q])
+                np.testing.assert_array_equal(rg[4][q, :c], ro[4][q, :c])
+                np.testing.assert_array_equal(rg[2][q, :c], ro[2][q, :c])
+                for r in range(c):
+                    L = ro[4][q, r]
+                    assert np.array_equal(rg[3][q, r, :L], ro[3][q, r, :L])
+                    V = min(int(ro[2][q, r]), 8)
+                    assert np.array_equal(rg[1][q, r, :V], ro[1][q, r, :V])
+    finally:
+        g.close()
+
+
+def test_empty_batches_and_pool_exhaustion():
+    g = GpuIndex(8, pool_bytes=64 * 136 * 64)  # 4096 slabs
+    try:
+        # Zero-sized calls are no-ops.
+        z = np.zeros((0, 4), np.uint32)
+        g.t.insert(None, 4, None, None, 1, None, 0)
+        w = wl.c1(n_keys=20000, n_finds=10)
+        from indexingpu_b200 import MasstreeError
+        with pytest.raises(MasstreeError) as e:
+            g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        assert e.value.code == 1  # MT_ERR_OOM, reported, no hang
+        del z
+    finally:
+        g.close()
+
+
+@pytest.mark.skipif(not RefMasstree.available(), reason="reference build absent")
+def test_against_reference_c1_and_scan():
+    w = wl.c1(n_keys=30000, n_finds=30000)
+    g, r = GpuIndex(8), RefIndex(pool_ratio=0.02)
+    try:
+        g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        r.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        vg, lg = g.find(w["find_keys"], w["find_lens"], 2)
+        vr, lr = r.find(w["find_keys"], w["find_lens"], 2)
+        assert_found(vg, lg, vr, lr, "find vs reference")
+        w3 = wl.c3(30000, 2000)
+        g3, r3 = GpuIndex(8), RefIndex(pool_ratio=0.02)
+        try:
+            g3.insert(w3["keys"], w3["lens"], w3["vals"], w3["vlens"])
+            r3.insert(w3["keys"], w3["lens"], w3["vals"], w3["vlens"])
+            a = g3.scan(w3["lower"], w3["lower_lens"], 100, maxV=1)
+            b = r3.scan(w3["lower"], w3["lower_lens"], 100, maxV=1)
+            for x, y, name in zip(a, b, ["counts", "values", "value_lengths", "keys", "key_lengths"]):
+                np.testing.assert_array_equal(x, y, err_msg=f"scan {name} vs reference")
+        finally:
+            g3.close()
+            r3.close()
+    finally:
+        g.close()
+        r.close()
+
+
+@pytest.mark.skipif(not RefMasstree.available(), reason="reference build absent")
+def test_against_reference_mixed_touch_once():
+    c2 = wl.C2(n_preload=30000, n_prefixes=64)
+    keys, lens, vals, vlens = c2.keys(np.arange(30000))
+    g, r = GpuIndex(8), RefIndex(pool_ratio=0.02)
+    try:
+        g.insert(keys, lens, vals, vlens)
+        r.insert(keys, lens, vals, vlens)
+        for bt in _touch_once_batches(c2, 3, 10000):
+            gv, gl, gr = g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            rv, rl, rr = r.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            nf = bt["types"] != wl.REQ_FIND
+            np.testing.assert_array_equal(gr[nf], rr[nf], err_msg="mixed results vs reference")
+            assert_found(gv[~nf], gl[~nf], rv[~nf], rl[~nf], "mixed finds vs reference")
+        a = dump_via_scan(g, 16, 8, 200000)
+        b = dump_via_scan(r, 16, 8, 200000)
+        assert_same_state(a, b, "final state vs reference")
+    finally:
+        g.close()
+        r.close()
