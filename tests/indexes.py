@@ -1,16 +1,16 @@
 """Uniform numpy-in / numpy-out adapters over the three index implementations
-the tests compare: the CUDA library under test (GpuIndex), the CPU oracle
-(OracleIndex) and the reference's own gpu_masstree (RefIndex).
+the tests compare: the CUDA library under test (GpuIndex) and the CPU oracle
+(OracleIndex).
 
 keys are 2-D uint32 arrays (n, max_key_length); values (n, max_value_length).
 """
 import numpy as np
 
-from oracle.pyoracle import CpuOracle, RefMasstree
+from oracle.pyoracle import CpuOracle
 
 
 def _u32(a):
-    return np.ascontiguousarray(a, dtype=np.uint32)
+    return None if a is None else np.ascontiguousarray(a, dtype=np.uint32)
 
 
 class OracleIndex:
@@ -77,7 +77,7 @@ class OracleIndex:
 
 
 class _TorchIndex:
-    """Shared device-buffer plumbing for GpuIndex and RefIndex."""
+    """Device-buffer plumbing."""
 
     def __init__(self):
         import torch
@@ -173,81 +173,5 @@ class GpuIndex(_TorchIndex):
                     None if upper is None else self.d(_u32(upper)),
                     None if upper_lens is None else self.d(_u32(upper_lens)), counts, vals, maxV, vlens, okeys,
                     oklens, concurrent=concurrent)
-        self.t.sync()
-        return self.h(counts), self.h(vals), self.h(vlens), self.h(okeys), self.h(oklens)
-
-
-class RefIndex(_TorchIndex):
-    """The reference's gpu_masstree.  Its insert/update/erase report nothing,
-    so those return None."""
-    name = "reference"
-
-    def __init__(self, pool_ratio=0.02):
-        super().__init__()
-        self.t = RefMasstree(pool_ratio)
-
-    def close(self):
-        self.t.close()
-
-    def insert(self, keys, klens, vals, vlens, n=None, upsert=False):
-        assert not upsert
-        keys, vals = _u32(keys), _u32(vals)
-        n = len(keys) if n is None else n
-        self.t.insert(self.d(keys), keys.shape[1], self.d(_u32(klens)), self.d(vals), vals.shape[1],
-                      self.d(_u32(vlens)), n)
-        self.t.sync()
-        return None
-
-    def update(self, keys, klens, vals, vlens, n=None):
-        keys, vals = _u32(keys), _u32(vals)
-        n = len(keys) if n is None else n
-        self.t.update(self.d(keys), keys.shape[1], self.d(_u32(klens)), self.d(vals), vals.shape[1],
-                      self.d(_u32(vlens)), n)
-        self.t.sync()
-        return None
-
-    def erase(self, keys, klens, n=None):
-        keys = _u32(keys)
-        n = len(keys) if n is None else n
-        self.t.erase(self.d(keys), keys.shape[1], self.d(_u32(klens)), n)
-        self.t.sync()
-        return None
-
-    def find(self, keys, klens, maxV, n=None, concurrent=False):
-        torch = self.torch
-        keys = _u32(keys)
-        n = len(keys) if n is None else n
-        vals = self.zeros((n, maxV), torch.uint32)
-        vlens = self.zeros(n, torch.uint32)
-        self.t.find(self.d(keys), keys.shape[1], self.d(_u32(klens)), vals, maxV, vlens, n, concurrent)
-        self.t.sync()
-        return self.h(vals), self.h(vlens)
-
-    def mixed(self, types, keys, klens, vals, vlens, n=None):
-        torch = self.torch
-        keys = _u32(keys)
-        n = len(keys) if n is None else n
-        dv = self.d(_u32(vals))
-        dvl = self.d(_u32(vlens))
-        res = self.zeros(n, torch.bool)
-        self.t.mixed(self.d(np.ascontiguousarray(types, np.uint8)), self.d(keys), keys.shape[1], self.d(_u32(klens)),
-                     dv, dv.shape[1], dvl, res, n)
-        self.t.sync()
-        return self.h(dv), self.h(dvl), self.h(res).astype(np.uint8)
-
-    def scan(self, lower, lower_lens, max_count, upper=None, upper_lens=None, maxV=1, nq=None):
-        torch = self.torch
-        lower = _u32(lower)
-        nq = len(lower) if nq is None else nq
-        maxK = lower.shape[1]
-        counts = self.zeros(nq, torch.uint32)
-        vals = self.zeros((nq, max_count, maxV), torch.uint32)
-        vlens = self.zeros((nq, max_count), torch.uint32)
-        okeys = self.zeros((nq, max_count, maxK), torch.uint32)
-        oklens = self.zeros((nq, max_count), torch.uint32)
-        self.t.scan(self.d(lower), self.d(_u32(lower_lens)), maxK, max_count, nq,
-                    None if upper is None else self.d(_u32(upper)),
-                    None if upper_lens is None else self.d(_u32(upper_lens)), upper is not None, counts, vals, maxV,
-                    vlens, okeys, oklens)
         self.t.sync()
         return self.h(counts), self.h(vals), self.h(vlens), self.h(okeys), self.h(oklens)

@@ -1,13 +1,12 @@
-"""Parity of the CUDA library with the CPU oracle and with the reference's own
-gpu_masstree on seeded workloads shaped like the benchmark configurations, at
-sizes the oracle finishes in seconds.  Integer results must match bit-for-bit.
+"""Parity of the CUDA library with the CPU oracle on seeded workloads shaped
+like the benchmark configurations, at sizes the oracle finishes in seconds.
+Integer results must match bit-for-bit.
 """
 import numpy as np
 import pytest
 
-from indexes import GpuIndex, OracleIndex, RefIndex
+from indexes import GpuIndex, OracleIndex
 from indexingpu_b200 import workload as wl
-from oracle.pyoracle import RefMasstree
 from scenarios import assert_found
 
 pytestmark = pytest.mark.gpu
@@ -210,52 +209,3 @@ def test_empty_batches_and_pool_exhaustion():
         del z
     finally:
         g.close()
-
-
-@pytest.mark.skipif(not RefMasstree.available(), reason="reference build absent")
-def test_against_reference_c1_and_scan():
-    w = wl.c1(n_keys=30000, n_finds=30000)
-    g, r = GpuIndex(8), RefIndex(pool_ratio=0.02)
-    try:
-        g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
-        r.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
-        vg, lg = g.find(w["find_keys"], w["find_lens"], 2)
-        vr, lr = r.find(w["find_keys"], w["find_lens"], 2)
-        assert_found(vg, lg, vr, lr, "find vs reference")
-        w3 = wl.c3(30000, 2000)
-        g3, r3 = GpuIndex(8), RefIndex(pool_ratio=0.02)
-        try:
-            g3.insert(w3["keys"], w3["lens"], w3["vals"], w3["vlens"])
-            r3.insert(w3["keys"], w3["lens"], w3["vals"], w3["vlens"])
-            a = g3.scan(w3["lower"], w3["lower_lens"], 100, maxV=1)
-            b = r3.scan(w3["lower"], w3["lower_lens"], 100, maxV=1)
-            for x, y, name in zip(a, b, ["counts", "values", "value_lengths", "keys", "key_lengths"]):
-                np.testing.assert_array_equal(x, y, err_msg=f"scan {name} vs reference")
-        finally:
-            g3.close()
-            r3.close()
-    finally:
-        g.close()
-        r.close()
-
-
-@pytest.mark.skipif(not RefMasstree.available(), reason="reference build absent")
-def test_against_reference_mixed_touch_once():
-    c2 = wl.C2(n_preload=30000, n_prefixes=64)
-    keys, lens, vals, vlens = c2.keys(np.arange(30000))
-    g, r = GpuIndex(8), RefIndex(pool_ratio=0.02)
-    try:
-        g.insert(keys, lens, vals, vlens)
-        r.insert(keys, lens, vals, vlens)
-        for bt in _touch_once_batches(c2, 3, 10000):
-            gv, gl, gr = g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
-            rv, rl, rr = r.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
-            nf = bt["types"] != wl.REQ_FIND
-            np.testing.assert_array_equal(gr[nf], rr[nf], err_msg="mixed results vs reference")
-            assert_found(gv[~nf], gl[~nf], rv[~nf], rl[~nf], "mixed finds vs reference")
-        a = dump_via_scan(g, 16, 8, 200000)
-        b = dump_via_scan(r, 16, 8, 200000)
-        assert_same_state(a, b, "final state vs reference")
-    finally:
-        g.close()
-        r.close()
