@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Mixed-batch throughput of the B200 masstree on the 16M variable-length-key
+workload (one step = one mixed_batch call of 1M requests: 50% find, 30% insert
+of fresh keys, 10% update, 10% erase, Zipf(0.99) key choice, after a 16M-key
+preload; keys 2-16 slices sharing 4096 four-slice prefixes, values 1-8 slices).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl ours (default) prints one JSON line with the device-resident throughput
+(`value`), the end-to-end throughput through the C ABI with host buffers copied
+in and results copied out every step (`e2e`), the roofline of the batch kernel,
+the CPU baseline and the SM clocks seen during the timed region.
+--impl reference times the CPU restatement of the path (the reference's own CPU
+counterpart, masstree-beta, is not available) with every host thread, on the
+same workload.  Under torchrun each rank runs an independent replica (the index
+is not partitioned across GPUs), so `value` is the sum over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from indexingpu_b200 import workload as wl  # noqa: E402
+
+MAXK, MAXV = 16, 8
+METRIC = "mixed-batch Mops/s @16M var-len keys"
+UNIT = "Mops/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--preload", type=int, default=1 << 24)
+    ap.add_argument("--batch", type=int, default=1 << 20)
+    ap.add_argument("--tile", type=int, default=8)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
+    return ap.parse_args()
+
+
+# ---- data --------------------------------------------------------------------------
+
+def gen_keys(c2, ids, threads=16):
+    chunks = np.array_split(ids, max(1, min(threads, len(ids) // 65536)))
+    with ThreadPoolExecutor(len(chunks)) as ex:
+        parts = list(ex.map(c2.keys, chunks))
+    return tuple(np.concatenate([p[i] for p in parts]) for i in range(4))
+
+
+def gen_batches(c2, first, count, n, threads=16):
+    with ThreadPoolExecutor(min(threads, count)) as ex:
+        return list(ex.map(lambda b: c2.batch(b, n), range(first, first + count)))
+
+
+def alg_bytes(bt, vlen_out, results):
+    """Compulsory-traffic model per request (bytes): request I/O plus one
+    128-byte border line and, for a hit on a chained entry, one 128-byte suffix
+    line; successful insert/update/erase count their lines twice (read and
+    write back).  Interior levels are assumed L2-resident."""
+    t = bt["types"]
+    L = bt["lens"].astype(np.int64)
+    vin = bt["vlens"].astype(np.int64)
+    req = 4 * L + 4 + 1
+    find = t == wl.REQ_FIND
+    io = np.where(find, 4 * np.minimum(vlen_out.astype(np.int64), MAXV) + 4, 1)
+    io = io + np.where((t == wl.REQ_INSERT) | (t == wl.REQ_UPDATE), 4 * vin + 4, 0)
+    hit = np.where(find, vlen_out > 0, results.astype(bool))
+    vl = np.where(find, vlen_out.astype(np.int64), vin)
+    chained = hit & ((vl > 1) | (L >= 6))
+    lines = 128 * (1 + chained.astype(np.int64))
+    mut_ok = (~find) & results.astype(bool)
+    lines = np.where(mut_ok, 2 * lines, lines)
+    return int((req + io + lines).sum())
+
+
+# ---- clocks ------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_profile():
+    """Per-launch DRAM bytes of the batch kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "mixed_batch_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_request")
+    return None
+
+
+# ---- CPU leg (oracle port) -----------------------------------------------------------
+
+def cpu_run(preload_data, batches, threads):
+    """Times the range-partitioned multi-threaded CPU restatement (the oracle
+    port) on mixed batches after the same preload; returns Mops/s per batch."""
+    from oracle.pyoracle import CpuOracle
+    keys, lens, vals, vlens = preload_data
+    o = CpuOracle(shards=threads, threads=threads)
+    o.insert(keys, MAXK, lens, vals, MAXV, vlens, len(keys))
+    rates = []
+    for bt in batches:
+        v = bt["vals"].copy()
+        vl = bt["vlens"].copy()
+        res = np.zeros(len(bt["types"]), np.uint8)
+        t0 = time.perf_counter()
+        o.mixed(bt["types"], bt["keys"], MAXK, bt["lens"], v, MAXV, vl, res, len(bt["types"]))
+        dt = time.perf_counter() - t0
+        rates.append(len(bt["types"]) / dt / 1e6)
+    del o
+    return rates
+
+
+# ---- GPU leg -------------------------------------------------------------------------
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from indexingpu_b200 import GpuMasstree
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    c2 = wl.C2(n_preload=args.preload, seed=0xC2 + rank)
+    pre = gen_keys(c2, np.arange(args.preload))
+    nb = args.warmup + args.steps
+    batches = gen_batches(c2, 0, nb, args.batch)
+    e2e_w, e2e_k = 2, max(1, min(args.e2e_steps, args.steps))
+    e2e_batches = gen_batches(c2, nb, e2e_w + e2e_k, args.batch)
+
+    tree = GpuMasstree(pool_ratio=0.6, tile_size=args.tile)
+    if args.blocks_per_sm:
+        tree.set_blocks_per_sm(args.blocks_per_sm)
+    stream = torch.cuda.current_stream()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    # Preload in 1M chunks.
+    pk = d(pre[0]); pl = d(pre[1]); pv = d(pre[2]); pvl = d(pre[3])
+    for s in range(0, args.preload, 1 << 20):
+        e = min(args.preload, s + (1 << 20))
+        tree.insert(pk[s:e], MAXK, pl[s:e], pv[s:e], MAXV, pvl[s:e], e - s, stream=stream)
+    tree.sync(stream)
+    del pk, pl, pv, pvl
+
+    # Device-resident batches.
+    dev_b = []
+    for bt in batches:
+        dev_b.append(dict(types=d(bt["types"]), keys=d(bt["keys"]), lens=d(bt["lens"]), vals=d(bt["vals"]),
+                          vlens=d(bt["vlens"]), res=torch.zeros(args.batch, dtype=torch.bool, device="cuda")))
+    torch.cuda.synchronize()
+
+    def step(b):
+        tree.mixed_batch(b["types"], b["keys"], MAXK, b["lens"], b["vals"], MAXV, b["vlens"], b["res"], args.batch,
+                         stream=stream)
+
+    for i in range(args.warmup):
+        step(dev_b[i])
+    tree.sync(stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step(dev_b[args.warmup + i])
+        ev[i][1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    tree.sync(stream)
+    total_ms = t0.elapsed_time(t1)
+    per_step = [a.elapsed_time(b) for a, b in ev]
+
+    # Algorithmic bytes from the timed batches' own outcomes.
+    abytes = 0
+    for i in range(args.steps):
+        b = dev_b[args.warmup + i]
+        bt = batches[args.warmup + i]
+        abytes += alg_bytes(bt, b["vlens"].cpu().numpy(), b["res"].cpu().numpy())
+    del dev_b
+
+    # End to end: pinned host buffers in, results out, every step.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    host = [dict(types=pin(bt["types"]), keys=pin(bt["keys"]), lens=pin(bt["lens"]), vals=pin(bt["vals"]),
+                 vlens=pin(bt["vlens"])) for bt in e2e_batches]
+    out = dict(vals=torch.empty((args.batch, MAXV), dtype=torch.uint32).pin_memory(),
+               vlens=torch.empty(args.batch, dtype=torch.uint32).pin_memory(),
+               res=torch.empty(args.batch, dtype=torch.bool).pin_memory())
+    dbuf = dict(types=torch.empty(args.batch, dtype=torch.uint8, device="cuda"),
+                keys=torch.empty((args.batch, MAXK), dtype=torch.uint32, device="cuda"),
+                lens=torch.empty(args.batch, dtype=torch.uint32, device="cuda"),
+                vals=torch.empty((args.batch, MAXV), dtype=torch.uint32, device="cuda"),
+                vlens=torch.empty(args.batch, dtype=torch.uint32, device="cuda"),
+                res=torch.empty(args.batch, dtype=torch.bool, device="cuda"))
+    h2d = sum(host[0][k].numel() * host[0][k].element_size() for k in host[0])
+    d2h = sum(out[k].numel() * out[k].element_size() for k in out)
+
+    def e2e_step(h):
+        for k in ("types", "keys", "lens", "vals", "vlens"):
+            dbuf[k].copy_(h[k], non_blocking=True)
+        tree.mixed_batch(dbuf["types"], dbuf["keys"], MAXK, dbuf["lens"], dbuf["vals"], MAXV, dbuf["vlens"],
+                         dbuf["res"], args.batch, stream=stream)
+        for k in ("vals", "vlens", "res"):
+            out[k].copy_(dbuf[k], non_blocking=True)
+
+    for i in range(e2e_w):
+        e2e_step(host[i])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_k):
+        e2e_step(host[e2e_w + i])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tree.sync(stream)
+    e2e_ms = e0.elapsed_time(e1)
+    stats = tree.stats()
+    tree.close()
+
+    # Reduce over ranks: max time.
+    if dist:
+        t = torch.tensor([total_ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+    reqs = args.steps * args.batch * world
+    value = reqs / (total_ms / 1e3) / 1e6
+    e2e_value = e2e_k * args.batch * world / (e2e_ms / 1e3) / 1e6
+
+    res = None
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        kern_s = statistics.mean(per_step) / 1e3
+        achieved = abytes / args.steps / kern_s / 1e9
+        tr = traffic_profile()
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            cpu_b = gen_batches(c2, 0, args.cpu_batches, args.batch)
+            rates = cpu_run(pre, cpu_b, threads)
+            cpu = {"value": round(statistics.mean(rates), 3), "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_batches} mixed batches of {args.batch} requests after the "
+                             f"{args.preload}-key preload, range-partitioned std::map restatement, "
+                             f"{threads} threads"}
+        sorted_steps = sorted(per_step)
+        res = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded, counter-based)",
+            "config": {"workload": "mixed_batch 1M requests (50/30/10/10 find/insert/update/erase, Zipf 0.99) "
+                                   "after a 16M-key preload; keys 2-16 slices, 4096 shared prefixes; values 1-8 slices",
+                       "preload_keys": args.preload, "batch_requests": args.batch, "max_key_length": MAXK,
+                       "max_value_length": MAXV, "tile_size": args.tile, "form": "plain per-call mixed_batch",
+                       "l2": "no flush: the index (>2 GB of slabs) and each batch's inputs exceed the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "batch_latency_ms": {"p50": round(sorted_steps[len(sorted_steps) // 2], 4),
+                                 "p99": round(sorted_steps[min(len(sorted_steps) - 1,
+                                                               int(0.99 * len(sorted_steps)))], 4)},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_k},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": None if tr is None else int(tr * args.batch),
+                         "algorithmic_bytes_per_step": abytes // args.steps,
+                         "kernel": "batch_kernel<T, mixed> (+ reclaim_kernel)"},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": 2 * args.steps,
+            "pool": {"used_slabs": stats["used_slabs"], "total_slabs": stats["total_slabs"]},
+        }
+    return res
+
+
+def run_reference(args, rank):
+    """CPU restatement timed with every host thread (bounded per-step sample)."""
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    c2 = wl.C2(n_preload=args.preload, seed=0xC2)
+    pre = gen_keys(c2, np.arange(args.preload))
+    batches = gen_batches(c2, 0, args.warmup + args.steps, args.batch)
+    from oracle.pyoracle import CpuOracle
+    o = CpuOracle(shards=threads, threads=threads)
+    o.insert(pre[0], MAXK, pre[1], pre[2], MAXV, pre[3], args.preload)
+    times = []
+    for i, bt in enumerate(batches):
+        v, vl = bt["vals"].copy(), bt["vlens"].copy()
+        res = np.zeros(args.batch, np.uint8)
+        t0 = time.perf_counter()
+        o.mixed(bt["types"], bt["keys"], MAXK, bt["lens"], v, MAXV, vl, res, args.batch)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = args.steps * args.batch / total / 1e6
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded, counter-based)",
+            "config": {"workload": "mixed_batch 1M requests (50/30/10/10 find/insert/update/erase, Zipf 0.99) "
+                                   "after a 16M-key preload; keys 2-16 slices, 4096 shared prefixes; values 1-8 slices",
+                       "preload_keys": args.preload, "batch_requests": args.batch},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} timed mixed batches of {args.batch} requests; CPU restatement "
+                                       "(range-partitioned std::map, one thread per shard); the reference's own "
+                                       "CPU path (masstree-beta) is absent and its GPU gpu_masstree hung on B200"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            res = run_reference(args, rank)
+        else:
+            res = run_ours(args, rank, world, dist)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
