@@ -125,6 +125,21 @@ int mt_stats(mt_masstree* tree, mt_stats_t* out);
  * every call).  Retired slabs are those unlinked by earlier calls. */
 int mt_reclaim(mt_masstree* tree, void* stream);
 
+/* Structural check of the whole index from a device snapshot (synchronous):
+ * node counts, key order inside and across nodes, separators equal to child
+ * high keys, suffix chain lengths, no node left locked.  num_keys receives the
+ * number of stored keys; msg (may be NULL) a one-line report.  Returns MT_OK
+ * or MT_ERR_CORRUPT.  Reference gpu_masstree::validate (gpu_masstree.hpp:1421-1472). */
+int mt_validate(mt_masstree* tree, uint64_t* num_keys, char* msg, size_t msg_len);
+
+/* Self-test of the assumption that one tile's 128-byte node load observes a
+ * node store atomically, at the given tile width: writer tiles publish lines
+ * of identical words while reader tiles count lines whose words disagree.
+ * Allocates its own buffers; bounded by iters.  New in this library (the
+ * reference states the assumption in README.md:168-172 without a test). */
+int mt_selftest_line_atomicity(uint32_t tile_size, uint32_t nlines, uint32_t iters, uint64_t* reads,
+                               uint64_t* torn);
+
 /* Human-readable name of a status code. */
 const char* mt_status_string(int status);
 

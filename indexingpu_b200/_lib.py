@@ -27,6 +27,8 @@ SIGNATURES = {
     "mt_stats": (_int, [_p, _p]),
     "mt_reclaim": (_int, [_p, _p]),
     "mt_status_string": (ctypes.c_char_p, [_int]),
+    "mt_validate": (_int, [_p, ctypes.POINTER(_u64), ctypes.c_char_p, ctypes.c_size_t]),
+    "mt_selftest_line_atomicity": (_int, [_u32, _u32, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
 }
 
 

@@ -17,7 +17,9 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "mt_tree.cuh"
 #include "../../include/mt_masstree.h"
@@ -168,6 +170,47 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(tree_view tv, scan_args a)
       if (t.rank == r) cnt = c;
     }
     if (i < a.n && a.counts) a.counts[i] = cnt;
+  }
+}
+
+
+// Line-atomicity self-test: writer tiles publish whole 128-byte lines whose
+// words all carry one stamp, reader tiles load lines the way node loads do
+// and count lines whose words disagree (a torn read).  Both loops are bounded.
+template <int T>
+__global__ void line_atomicity_kernel(uint32_t* lines, uint32_t nlines, uint32_t iters,
+                                      unsigned long long* reads, unsigned long long* torn) {
+  tile<T> t;
+  constexpr int W = 32 / T;
+  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
+  const bool writer = (tile_id & 1u) == 0u;
+  unsigned long long my_reads = 0, my_torn = 0;
+  uint32_t x = tile_id * 0x9E3779B1u + 1u;
+  for (uint32_t it = 0; it < iters; ++it) {
+    x ^= x << 13; x ^= x >> 17; x ^= x << 5;
+    const uint32_t line = t.shfl(x, 0) % nlines;
+    uint32_t* base = lines + (size_t)line * 32u + t.rank * W;
+    uint32_t w[W];
+    if (writer) {
+      const uint32_t stamp = (tile_id << 12) ^ it;
+#pragma unroll
+      for (int k = 0; k < W; ++k) w[k] = stamp;
+      t.sync();
+      store_words<W, st_order::RELEASE>(base, w);
+    } else {
+      load_words<W, kConc>(base, w);
+      uint32_t lo = w[0], hi = w[0];
+#pragma unroll
+      for (int k = 1; k < W; ++k) { lo = min(lo, w[k]); hi = max(hi, w[k]); }
+      lo = t.min_all(lo);
+      hi = __reduce_max_sync(t.mask, hi);
+      my_reads += 1;
+      my_torn += (lo != hi) ? 1 : 0;
+    }
+  }
+  if (t.leader() && !writer) {
+    atomicAdd(reads, my_reads);
+    atomicAdd(torn, my_torn);
   }
 }
 
@@ -533,3 +576,148 @@ const char* mt_status_string(int s) {
 }
 
 }  // extern "C"
+
+// ---- validation (host walk over a device snapshot) ----------------------------------
+
+namespace {
+
+struct validator {
+  const std::vector<uint32_t>& img;  // slab words
+  uint32_t nslabs;
+  uint64_t keys = 0, nodes = 0, chains = 0;
+  std::string err;
+  int depth_limit = 1 << 16;
+
+  const uint32_t* slab(uint32_t i) const { return img.data() + (size_t)i * 32u; }
+  bool ok(uint32_t i) { return i < nslabs; }
+  bool fail(const std::string& m) {
+    if (err.empty()) err = m;
+    return false;
+  }
+
+  bool chain(uint32_t head) {
+    if (!ok(head)) return fail("suffix chain head out of range");
+    const uint32_t hdr = slab(head)[SUF_WORD_HDR];
+    const uint32_t kl = hdr & kMaxLen16, vl = hdr >> 16;
+    const uint32_t need = suf_nodes(kl, vl);
+    uint32_t c = head;
+    for (uint32_t n = 1; n < need; ++n) {
+      c = slab(c)[SUF_WORD_NEXT];
+      if (!ok(c)) return fail("suffix chain shorter than its header");
+    }
+    if (slab(c)[SUF_WORD_NEXT] != kInvalid) return fail("suffix chain longer than its header");
+    ++chains;
+    return true;
+  }
+
+  // Validate the subtree at idx covering (lo, hi] (lo exclusive unless first).
+  bool subtree(uint32_t idx, uint64_t lo_excl, uint32_t hi, int level, int& border_level, int layer_depth) {
+    if (!ok(idx)) return fail("node index out of range");
+    const uint32_t* w = slab(idx);
+    const uint32_t meta = w[WORD_META], ks = w[WORD_KS], n = meta & META_COUNT;
+    ++nodes;
+    if (meta & META_LOCK) return fail("node left locked");
+    if (n > (uint32_t)kMaxEntries) return fail("count above 14");
+    if (w[WORD_HIGH] != hi) return fail("high key differs from the parent's separator");
+    const bool border = (meta & META_BORDER) != 0;
+    if (border) {
+      if (border_level < 0) border_level = level;
+      else if (border_level != level) return fail("border nodes at different depths");
+      uint64_t prev = 0;
+      bool have = false;
+      for (uint32_t e = 0; e < n; ++e) {
+        const uint32_t k = w[2 * e], v = w[2 * e + 1], st = ks_get(ks, e);
+        const uint64_t pos = ((uint64_t)k << 1) | (ks_more(st) ? 1u : 0u);
+        if (have && pos <= prev) return fail("border entries out of order");
+        if (lo_excl != ~0ull && (uint64_t)k <= lo_excl) return fail("border key below its range");
+        if (k > hi) return fail("border key above its high key");
+        prev = pos;
+        have = true;
+        if (st == KS_LINK) {
+          if (!layer(v, layer_depth + 1)) return false;
+        } else if (st == KS_VALUE) {
+          ++keys;
+        } else {
+          if (!chain(v)) return false;
+          ++keys;
+        }
+      }
+      return true;
+    }
+    if (n == 0) return fail("empty interior node");
+    uint64_t lo = lo_excl;
+    for (uint32_t e = 0; e < n; ++e) {
+      const uint32_t sep = w[2 * e];
+      if (lo != ~0ull && (uint64_t)sep <= lo) return fail("interior separators out of order");
+      if (!subtree(w[2 * e + 1], lo, sep, level + 1, border_level, layer_depth)) return false;
+      lo = sep;
+    }
+    if (w[2 * (n - 1)] != hi) return fail("last separator differs from the high key");
+    return true;
+  }
+
+  bool layer(uint32_t root, int depth) {
+    if (depth > depth_limit) return fail("trie deeper than the limit");
+    if (!ok(root)) return fail("layer root out of range");
+    if (!(slab(root)[WORD_META] & META_ROOT)) return fail("layer root without ROOT flag");
+    int border_level = -1;
+    return subtree(root, ~0ull, 0xFFFFFFFFu, 0, border_level, depth);
+  }
+};
+
+}  // namespace
+
+extern "C" int mt_validate(mt_masstree* t, uint64_t* num_keys, char* msg, size_t msg_len) {
+  if (!t) return MT_ERR_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return MT_ERR_CUDA;
+  const pool_view& p = t->tv.pool;
+  std::vector<uint32_t> img((size_t)p.num_slabs * 32u, 0u);
+  const size_t nctr = (size_t)p.num_shards * 3u * kCtrStride;
+  std::vector<int> h(nctr);
+  if (cudaMemcpy(h.data(), p.ctr, nctr * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_CUDA;
+  for (uint32_t s = 0; s < p.num_shards; ++s) {
+    const int bump = std::min<int>(std::max(h[(3 * s + 1) * kCtrStride], 0), (int)p.shard_slabs);
+    if (bump == 0) continue;
+    const size_t off = (size_t)s * p.shard_slabs * 32u;
+    if (cudaMemcpy(img.data() + off, p.slabs + off, (size_t)bump * 128u, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return MT_ERR_CUDA;
+  }
+  validator v{img, p.num_slabs};
+  const bool good = v.layer(t->tv.root, 0);
+  if (num_keys) *num_keys = v.keys;
+  if (msg && msg_len) {
+    std::snprintf(msg, msg_len, "%s (keys %llu, nodes %llu, chains %llu)", good ? "ok" : v.err.c_str(),
+                  (unsigned long long)v.keys, (unsigned long long)v.nodes, (unsigned long long)v.chains);
+  }
+  return good ? MT_OK : MT_ERR_CORRUPT;
+}
+
+extern "C" int mt_selftest_line_atomicity(uint32_t tile_size, uint32_t nlines, uint32_t iters, uint64_t* reads,
+                                          uint64_t* torn) {
+  if (!valid_tile(tile_size) || nlines == 0 || !reads || !torn) return MT_ERR_INVALID_ARG;
+  uint32_t* lines = nullptr;
+  unsigned long long* ctr = nullptr;
+  if (cudaMalloc(&lines, (size_t)nlines * 128u) != cudaSuccess) return MT_ERR_CUDA;
+  if (cudaMalloc(&ctr, 2 * sizeof(unsigned long long)) != cudaSuccess) { cudaFree(lines); return MT_ERR_CUDA; }
+  cudaMemset(lines, 0, (size_t)nlines * 128u);
+  cudaMemset(ctr, 0, 2 * sizeof(unsigned long long));
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = sms * 8;
+  switch (tile_size) {
+    case 4: line_atomicity_kernel<4><<<grid, kBlock>>>(lines, nlines, iters, ctr, ctr + 1); break;
+    case 8: line_atomicity_kernel<8><<<grid, kBlock>>>(lines, nlines, iters, ctr, ctr + 1); break;
+    case 16: line_atomicity_kernel<16><<<grid, kBlock>>>(lines, nlines, iters, ctr, ctr + 1); break;
+    default: line_atomicity_kernel<32><<<grid, kBlock>>>(lines, nlines, iters, ctr, ctr + 1); break;
+  }
+  unsigned long long hctr[2] = {0, 0};
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(hctr, ctr, sizeof(hctr), cudaMemcpyDeviceToHost);
+  cudaFree(lines);
+  cudaFree(ctr);
+  if (e != cudaSuccess) return MT_ERR_CUDA;
+  *reads = hctr[0];
+  *torn = hctr[1];
+  return MT_OK;
+}

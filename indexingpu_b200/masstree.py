@@ -151,7 +151,26 @@ class GpuMasstree:
     def reclaim(self, stream=0):
         self._check(self._lib.mt_reclaim(self._h, _stream(stream)), "mt_reclaim")
 
+    def validate(self):
+        """Structural check of the whole index; returns (ok, num_keys, report)."""
+        n = ctypes.c_uint64()
+        buf = ctypes.create_string_buffer(512)
+        rc = self._lib.mt_validate(self._h, ctypes.byref(n), buf, 512)
+        if rc not in (0, 3):
+            self._check(rc, "mt_validate")
+        return rc == 0, int(n.value), buf.value.decode()
+
     def stats(self):
         s = _lib.MtStats()
         self._check(self._lib.mt_stats(self._h, ctypes.byref(s)), "mt_stats")
         return {f: getattr(s, f) for f, _ in _lib.MtStats._fields_}
+
+
+def line_atomicity_selftest(tile_size, nlines=64, iters=20000):
+    """(reads, torn reads) of the 128-byte line-atomicity self-test."""
+    lib = _lib.load()
+    r, t = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib.mt_selftest_line_atomicity(tile_size, nlines, iters, ctypes.byref(r), ctypes.byref(t))
+    if rc != 0:
+        raise MasstreeError(rc, "mt_selftest_line_atomicity")
+    return int(r.value), int(t.value)
