@@ -388,6 +388,7 @@ int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
   root_img[WORD_SIB] = kInvalid;
   root_img[WORD_META] = META_BORDER | META_ROOT;
   root_img[WORD_KS] = 0u;
+  root_img[WORD_CSUM] = node_checksum(root_img);
   const int one = 1;
   if (e == cudaSuccess) e = cudaMemcpy(p.slabs, root_img, sizeof(root_img), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(p.bump(0), &one, sizeof(int), cudaMemcpyHostToDevice);
@@ -617,7 +618,8 @@ struct validator {
     const uint32_t meta = w[WORD_META], ks = w[WORD_KS], n = meta & META_COUNT;
     ++nodes;
     if (meta & META_LOCK) return fail("node left locked");
-    if (n > (uint32_t)kMaxEntries) return fail("count above 14");
+    if (n > (uint32_t)kMaxEntries) return fail("count above the node capacity");
+    if (node_checksum(w) != w[WORD_CSUM]) return fail("node checksum mismatch");
     if (w[WORD_HIGH] != hi) return fail("high key differs from the parent's separator");
     const bool border = (meta & META_BORDER) != 0;
     if (border) {

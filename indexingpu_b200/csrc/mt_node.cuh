@@ -1,15 +1,25 @@
 // B-link tree node of one trie layer, held in registers by a tile.
 //
-// One node is one 128-byte slab = 32 u32 words = 16 (key, value) pairs:
-//   entries 0..13 : word 2e = key slice, word 2e+1 = value
+// One node is one 128-byte slab = 32 u32 words:
+//   entries 0..12 : word 2e = key slice, word 2e+1 = value
 //                   border node  : value = inline value / suffix slab / layer root
 //                   interior node: key = separator (largest slice routed to the
 //                                  child), value = child slab
+//   word 26       : checksum of the other 31 words (LOCK bit masked)
+//   word 27       : reserved (0)
 //   word 28       : high key (largest slice this node covers; 0xFFFFFFFF for the
 //                   rightmost node of a level)
 //   word 29       : right sibling slab (valid iff META_SIB)
 //   word 30       : meta  = count:4 | LOCK | BORDER | SIB | ROOT | version:16 (bits 16..31)
 //   word 31       : keystates of a border node, 2 bits per entry
+//
+// Why a checksum: on B200 a 128-byte line stored by one warp instruction is
+// NOT always observed atomically by a concurrent 128-byte load (the line
+// self-test, mt_selftest_line_atomicity, counts torn reads at every tile width,
+// about 1 in 10^5 reads under contention).  Lock-free readers therefore verify
+// the checksum and reload on a mismatch; writers recompute it on every publish.
+// The reference keeps the same defence behind a switch that is compiled out
+// (include/compute_hash.hpp:179-199) and relies on atomicity instead.
 //
 // Keystate (bit0 = "key continues past this slice", bit1 = "value is a slab"):
 //   VALUE 00 : key ends here, value is the inline u32 value (value length 1)
@@ -29,7 +39,8 @@
 
 namespace mtb {
 
-constexpr int kMaxEntries = 14;
+constexpr int kMaxEntries = 13;
+constexpr uint32_t kTornRetries = 1u << 12;  // reloads of a torn node image before MT_ERR_CORRUPT
 constexpr uint32_t KS_VALUE = 0u, KS_LINK = 1u, KS_LONGVAL = 2u, KS_SUFFIX = 3u;
 constexpr uint32_t KS_MORE = 1u, KS_SLAB = 2u;
 
@@ -40,7 +51,29 @@ constexpr uint32_t META_SIB = 1u << 6;
 constexpr uint32_t META_ROOT = 1u << 7;
 constexpr uint32_t META_VERSION_ONE = 1u << 16;
 
-constexpr int WORD_HIGH = 28, WORD_SIB = 29, WORD_META = 30, WORD_KS = 31;
+constexpr int WORD_CSUM = 26, WORD_HIGH = 28, WORD_SIB = 29, WORD_META = 30, WORD_KS = 31;
+
+// lowbias32 integer hash (C. Wellons, "Prospecting for Hash Functions", 2018).
+MT_HD uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  x *= 0x846CA68Bu;
+  x ^= x >> 16;
+  return x;
+}
+// Contribution of word g (value v) to a node checksum.
+MT_HD uint32_t csum_term(uint32_t g, uint32_t v) {
+  if (g == (uint32_t)WORD_CSUM) return 0u;
+  if (g == (uint32_t)WORD_META) v &= ~(1u << 4);  // LOCK bit changes without a republish
+  return mix32(v ^ (g * 0x9E3779B9u) ^ 0x5BD1E995u);
+}
+// Host/device checksum of a full 32-word node image.
+MT_HD uint32_t node_checksum(const uint32_t* w) {
+  uint32_t h = 0;
+  for (uint32_t g = 0; g < 32u; ++g) h += csum_term(g, w[g]);
+  return h;
+}
 
 MT_HD uint32_t ks_get(uint32_t ks, uint32_t e) { return (ks >> (2u * e)) & 3u; }
 MT_HD bool ks_more(uint32_t state) { return (state & KS_MORE) != 0u; }
@@ -112,6 +145,26 @@ struct node {
   MT_DEV void clear_words() {
 #pragma unroll
     for (int k = 0; k < W; ++k) w[k] = 0u;
+  }
+  MT_DEV uint32_t tile_checksum(const tile<T>& t) const {
+    uint32_t h = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) h += csum_term(t.rank * W + k, w[k]);
+    return t.add_all(h);
+  }
+  // Write the checksum word of the current image (call after encode_header).
+  MT_DEV void seal(const tile<T>& t) { set_word(t, WORD_CSUM, tile_checksum(t)); }
+  // Load an image that concurrent writers may be publishing: reload until the
+  // checksum matches (bounded), else record corruption.
+  template <ld_order O>
+  MT_DEV bool load_verified(const tile<T>& t, const pool_view& p, uint32_t i) {
+    for (uint32_t r = 0; r < kTornRetries; ++r) {
+      load<O>(t, p, i);
+      if constexpr (O == ld_order::NC) return true;
+      if (tile_checksum(t) == word(t, WORD_CSUM)) return true;
+    }
+    if (t.leader()) record_error(p, ERR_CORRUPT);
+    return false;
   }
 
   // ---- entry queries --------------------------------------------------------
@@ -256,12 +309,12 @@ struct node {
       w[k] = (g < lim) ? v : 0u;
     }
   }
-  // Keep entries [0, p): clear words [2p, 28).
+  // Keep entries [0, p): clear the entry words [2p, 26).
   MT_DEV void truncate(const tile<T>& t, uint32_t p) {
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const uint32_t g = t.rank * W + k;
-      if (g >= 2u * p && g < (uint32_t)WORD_HIGH) w[k] = 0u;
+      if (g >= 2u * p && g < (uint32_t)WORD_CSUM) w[k] = 0u;
     }
   }
 };

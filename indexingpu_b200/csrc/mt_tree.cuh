@@ -12,10 +12,13 @@
 //   * scan visits keys in lexicographic u32-slice order (a key that is a prefix
 //     of another sorts first), both bounds inclusive.
 //
-// Concurrency: readers are lock-free and rely on a whole node being read by one
-// coalesced 128-byte access (the reference's assumption, README.md:168-172).
-// Writers lock a node through its meta word, publish the new node image with
-// release stores and release the lock with a separate release atomic.  Inserts
+// Concurrency: readers are lock-free.  The reference assumes one coalesced
+// 128-byte load observes a concurrent 128-byte store atomically
+// (README.md:168-172); on B200 that assumption fails about once in 10^5
+// contended reads, so every lock-free node load here is checked against the
+// node's checksum and reloaded on a mismatch (mt_node.cuh).  Writers lock a
+// node through its meta word, publish the new node image with release stores
+// and release the lock with a separate release atomic.  Inserts
 // split full nodes top-down on the way to the border node (the proactive
 // B-link split of Awad et al., "Engineering a High-Performance GPU B-Tree",
 // PPoPP 2019, which the reference also uses, include/gpu_masstree.hpp:1020-1148).
@@ -50,6 +53,13 @@ struct tree_view {
 // ---- locking -----------------------------------------------------------------
 
 template <int T>
+MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
+  t.sync();
+  if (t.leader()) atom_and_release(p.addr(idx) + WORD_META, ~META_LOCK);
+  t.sync();
+}
+
+template <int T>
 MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T>& nd) {
   uint32_t* mw = p.addr(idx) + WORD_META;
   for (uint32_t it = 0; it < kLockSpins; ++it) {
@@ -58,8 +68,9 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
     old = t.shfl(old, 0);
     if (!(old & META_LOCK)) {
       t.sync();
-      nd.template load<ld_order::ACQUIRE>(t, p, idx);
-      return true;
+      // No writer can publish this node while we hold its lock; a checksum
+      // mismatch here would be a bug, reported as corruption.
+      return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
     __nanosleep(32u << (it < 5u ? it : 5u));
@@ -68,18 +79,12 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
   return false;
 }
 
-template <int T>
-MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
-  t.sync();
-  if (t.leader()) atom_and_release(p.addr(idx) + WORD_META, ~META_LOCK);
-  t.sync();
-}
-
 // Publish the node image; the stored meta keeps LOCK set.
 template <int T>
 MT_DEV void publish_locked(const tile<T>& t, const pool_view& p, node<T>& nd) {
   nd.meta = (nd.meta | META_LOCK) + META_VERSION_ONE;
   nd.encode_header(t);
+  nd.seal(t);
   nd.template store<st_order::RELEASE>(t, p);
 }
 
@@ -95,6 +100,7 @@ MT_DEV void publish_unlock(const tile<T>& t, const pool_view& p, node<T>& nd) {
 template <int T>
 MT_DEV void publish_new(const tile<T>& t, const pool_view& p, node<T>& nd) {
   nd.encode_header(t);
+  nd.seal(t);
   nd.template store<st_order::RELEASE>(t, p);
 }
 
@@ -121,7 +127,7 @@ MT_DEV bool descend(const tile<T>& t, const pool_view& p, uint32_t root, uint32_
       if (t.leader()) record_error(p, ERR_CORRUPT);
       return false;
     }
-    nd.template load<O>(t, p, idx);
+    if (!nd.template load_verified<O>(t, p, idx)) return false;
     if (nd.must_move_right(slice)) { idx = nd.sib; continue; }
     if (nd.is_border()) return true;
     const int c = nd.child_pos(t, slice);
@@ -182,7 +188,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
       if (t.leader()) record_error(p, ERR_CORRUPT);
       return -1;
     }
-    nd.template load<kConc>(t, p, idx);
+    if (!nd.template load_verified<kConc>(t, p, idx)) return -1;
     if (nd.must_move_right(slice)) { idx = nd.sib; continue; }
     if (nd.is_border() && more) {
       const int e = nd.match(t, slice, true);
@@ -225,7 +231,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
       node<T> ln;
       rn.take_upper_from(t, nd, sp);
       rn.idx = R;
-      rn.meta = (border ? META_BORDER : 0u) | (kMaxEntries - sp);
+      rn.meta = (border ? META_BORDER : 0u) | (nd.count() - sp);
       rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
       rn.high = nd.high;
       rn.sib = kInvalid;
@@ -285,7 +291,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
       }
       rn.take_upper_from(t, nd, sp);
       rn.idx = R;
-      rn.meta = (border ? META_BORDER : 0u) | (nd.meta & META_SIB) | (kMaxEntries - sp);
+      rn.meta = (border ? META_BORDER : 0u) | (nd.meta & META_SIB) | (nd.count() - sp);
       rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
       rn.high = nd.high;
       rn.sib = nd.sib;
@@ -783,7 +789,7 @@ MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t*
       if (utight && nd.high >= upper[layer]) return count;
       const uint32_t sib = nd.sib;
       if (!p.valid(sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
-      nd.template load<O>(t, p, sib);
+      if (!nd.template load_verified<O>(t, p, sib)) return count;
       start = 0;
       continue;
     }
@@ -802,10 +808,10 @@ MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t*
       continue;
     }
     if (!p.valid(f.node)) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
-    nd.template load<O>(t, p, f.node);
+    if (!nd.template load_verified<O>(t, p, f.node)) return count;
     while (nd.must_move_right(f.slice)) {
       if (!p.valid(nd.sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
-      nd.template load<O>(t, p, nd.sib);
+      if (!nd.template load_verified<O>(t, p, nd.sib)) return count;
     }
     start = __popc(nd.entry_mask(t, [&](uint32_t k, uint32_t) { return k <= f.slice; }));
   }
