@@ -47,6 +47,8 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
 #define MT_FLAG_CONCURRENT 1u       /* find/scan may run beside writers (reference template `concurrent`) */
 #define MT_FLAG_UPDATE_IF_EXISTS 2u /* insert overwrites an existing key (reference `update_if_exists`) */
 #define MT_FLAG_USE_UPPER_KEY 4u    /* scan stops after upper_keys (reference `use_upper_key`) */
+#define MT_FLAG_SINGLE_PASS 8u      /* mixed_batch: one kernel for every kind instead of
+                                       finds-then-writes passes (comparison switch) */
 
 typedef struct mt_stats_t {
   uint64_t total_slabs;     /* slabs in the pool (128 bytes each) */
@@ -72,6 +74,9 @@ int mt_destroy(mt_masstree* tree);
 /* Launch shape: lanes per request (4/8/16/32) and resident blocks per SM
  * (0 = as many as fit).  New in this library. */
 int mt_set_tile_size(mt_masstree* tree, uint32_t tile_size);
+/* Lanes per request for inserts, updates and erases only (mt_set_tile_size
+ * sets both widths). */
+int mt_set_write_tile_size(mt_masstree* tree, uint32_t tile_size);
 int mt_set_blocks_per_sm(mt_masstree* tree, uint32_t blocks_per_sm);
 
 /* Reference gpu_masstree::find (gpu_masstree.hpp:86-99). */

@@ -40,10 +40,39 @@ struct batch_args {
   const uint32_t* value_lengths_in;
   uint32_t* value_lengths_out;
   bool* results;
+  const uint32_t* index;  // optional request subset
+  const uint32_t* n_dev;  // optional device-side request count (with index)
   uint32_t max_key_length;
   uint32_t max_value_length;
   uint32_t n;
 };
+
+// Split a mixed batch into its finds and its writes (insert/update/erase):
+// one atomic per warp and class.  Order inside a class is arbitrary (requests
+// of one mixed batch have no defined order).  counts = {finds, writes}.
+__global__ void partition_kernel(const uint8_t* types, uint32_t n, uint32_t* find_idx, uint32_t* write_idx,
+                                 uint32_t* counts) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    const bool is_find = valid && types[i] == MT_REQ_FIND;
+    const bool is_write = valid && !is_find;
+    const uint32_t fm = __ballot_sync(0xFFFFFFFFu, is_find);
+    const uint32_t wm = __ballot_sync(0xFFFFFFFFu, is_write);
+    uint32_t fb = 0, wb = 0;
+    if (lane == 0) {
+      if (fm) fb = atomicAdd(counts, (uint32_t)__popc(fm));
+      if (wm) wb = atomicAdd(counts + 1, (uint32_t)__popc(wm));
+    }
+    fb = __shfl_sync(0xFFFFFFFFu, fb, 0);
+    wb = __shfl_sync(0xFFFFFFFFu, wb, 0);
+    const uint32_t below = (1u << lane) - 1u;
+    if (is_find) find_idx[fb + __popc(fm & below)] = i;
+    if (is_write) write_idx[wb + __popc(wm & below)] = i;
+  }
+}
 
 struct scan_args {
   const uint32_t* lower;
@@ -92,10 +121,14 @@ __global__ void __launch_bounds__(kBlock) batch_kernel(tree_view tv, batch_args 
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   slab_cache<T> cache;
   cache.init(tv.pool, tile_id);
-  for (uint32_t base = tile_id * T; base < a.n; base += num_tiles * T) {
+  // With a.index the kernel serves requests a.index[0 .. *a.n_dev) (a subset
+  // produced by partition_kernel); otherwise requests 0 .. a.n.
+  const uint32_t n = a.n_dev ? *a.n_dev : a.n;
+  for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
-    const uint32_t i = base + t.rank;
-    const bool valid = i < a.n;
+    const uint32_t pos = base + t.rank;
+    const bool valid = pos < n;
+    const uint32_t i = (valid && a.index) ? a.index[pos] : pos;
     uint32_t kind = 0, klen = 0, vlen = 0;
     if (valid) {
       if constexpr (OP == OP_MIXED) kind = a.types[i];
@@ -112,14 +145,15 @@ __global__ void __launch_bounds__(kBlock) batch_kernel(tree_view tv, batch_args 
     const bool bad = valid && (klen > a.max_key_length || vlen > a.max_value_length || kind > MT_REQ_UPDATE);
     if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
     uint32_t res = 0, vout = 0;
-    const uint32_t nreq = min((uint32_t)T, a.n - base);
+    const uint32_t nreq = min((uint32_t)T, n - base);
     for (uint32_t r = 0; r < nreq; ++r) {
       if (t.shfl((uint32_t)bad, (int)r)) continue;
+      const uint32_t j = t.shfl(i, (int)r);
       const uint32_t k = t.shfl(kind, (int)r);
       const uint32_t kl = t.shfl(klen, (int)r);
       const uint32_t vl = t.shfl(vlen, (int)r);
       uint32_t rr = 0, vo = 0;
-      run_request<T, OP, CONC>(t, tv, cache, a, base + r, k, kl, vl, rr, vo);
+      run_request<T, OP, CONC>(t, tv, cache, a, j, k, kl, vl, rr, vo);
       if (t.rank == r) { res = rr; vout = vo; }
     }
     if (valid) {
@@ -250,8 +284,11 @@ using namespace mtb;
 struct mt_masstree {
   int device = 0;
   int sms = 0;
-  uint32_t tile_size = 8;
-  uint32_t blocks_per_sm = 0;  // 0 = occupancy limit
+  uint32_t tile_size = 8;        // finds and scans
+  uint32_t write_tile_size = 8;  // inserts, updates, erases
+  uint32_t blocks_per_sm = 0;    // 0 = occupancy limit
+  uint32_t* split_idx = nullptr; // mixed-batch partition scratch
+  uint32_t split_cap = 0;
   void* mem = nullptr;
   tree_view tv{};
   scan_frame* frames = nullptr;
@@ -303,17 +340,64 @@ int launch_batch_t(mt_masstree* t, const batch_args& a, cudaStream_t s) {
 }
 
 template <int OP, bool CONC>
-int launch_batch(mt_masstree* t, const batch_args& a, cudaStream_t s) {
-  if (a.n == 0) return MT_OK;
-  int rc = launch_reclaim(t, s);
-  if (rc) return rc;
-  switch (t->tile_size) {
+int launch_batch_tile(mt_masstree* t, uint32_t tile, const batch_args& a, cudaStream_t s) {
+  switch (tile) {
     case 4: return launch_batch_t<4, OP, CONC>(t, a, s);
     case 8: return launch_batch_t<8, OP, CONC>(t, a, s);
     case 16: return launch_batch_t<16, OP, CONC>(t, a, s);
     case 32: return launch_batch_t<32, OP, CONC>(t, a, s);
     default: return MT_ERR_INVALID_ARG;
   }
+}
+
+template <int OP, bool CONC>
+int launch_batch(mt_masstree* t, const batch_args& a, cudaStream_t s) {
+  if (a.n == 0) return MT_OK;
+  int rc = launch_reclaim(t, s);
+  if (rc) return rc;
+  return launch_batch_tile<OP, CONC>(t, OP == OP_FIND ? t->tile_size : t->write_tile_size, a, s);
+}
+
+// Index scratch for split mixed batches (grown on demand, kept).
+int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
+  if (n <= t->split_cap) return MT_OK;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MT_ERR_CUDA;
+  if (t->split_idx) cudaFree(t->split_idx);
+  t->split_idx = nullptr;
+  t->split_cap = 0;
+  // [counts(32 words, one line)] [find indices n] [write indices n]
+  if (cudaMalloc(&t->split_idx, (32u + 2ull * n) * sizeof(uint32_t)) != cudaSuccess) return MT_ERR_OOM;
+  t->split_cap = n;
+  return MT_OK;
+}
+
+// A mixed batch as three launches: partition by kind, then every find with the
+// find tile width, then every write (insert/update/erase) with the write tile
+// width.  Finds and writes of one batch have no defined order, so serving the
+// finds first is one of the orders the reference allows; it removes the
+// find/write divergence between the tiles of a warp.
+int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
+  if (a.n == 0) return MT_OK;
+  int rc = ensure_split_scratch(t, a.n, s);
+  if (rc) return rc;
+  rc = launch_reclaim(t, s);
+  if (rc) return rc;
+  uint32_t* counts = t->split_idx;
+  uint32_t* find_idx = t->split_idx + 32;
+  uint32_t* write_idx = find_idx + a.n;
+  if (cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+  partition_kernel<<<std::max(1, std::min(t->sms * 8, (int)((a.n + 255) / 256))), 256, 0, s>>>(
+      a.types, a.n, find_idx, write_idx, counts);
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
+  batch_args f = a;
+  f.index = find_idx;
+  f.n_dev = counts;
+  rc = launch_batch_tile<OP_MIXED, true>(t, t->tile_size, f, s);
+  if (rc) return rc;
+  batch_args w = a;
+  w.index = write_idx;
+  w.n_dev = counts + 1;
+  return launch_batch_tile<OP_MIXED, true>(t, t->write_tile_size, w, s);
 }
 
 template <int T, bool CONC>
@@ -354,6 +438,7 @@ int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
   auto* t = new (std::nothrow) mt_masstree();
   if (!t) return MT_ERR_OOM;
   t->tile_size = tile_size;
+  t->write_tile_size = tile_size;
   if (cudaGetDevice(&t->device) != cudaSuccess ||
       cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, t->device) != cudaSuccess) {
     delete t;
@@ -422,6 +507,7 @@ int mt_destroy(mt_masstree* t) {
   if (!t) return MT_ERR_INVALID_ARG;
   cudaDeviceSynchronize();
   if (t->frames) cudaFree(t->frames);
+  if (t->split_idx) cudaFree(t->split_idx);
   if (t->mem) cudaFree(t->mem);
   if (t->h_err) cudaFreeHost(t->h_err);
   delete t;
@@ -431,6 +517,13 @@ int mt_destroy(mt_masstree* t) {
 int mt_set_tile_size(mt_masstree* t, uint32_t ts) {
   if (!t || !valid_tile(ts)) return MT_ERR_INVALID_ARG;
   t->tile_size = ts;
+  t->write_tile_size = ts;
+  return MT_OK;
+}
+
+int mt_set_write_tile_size(mt_masstree* t, uint32_t ts) {
+  if (!t || !valid_tile(ts)) return MT_ERR_INVALID_ARG;
+  t->write_tile_size = ts;
   return MT_OK;
 }
 
@@ -489,7 +582,8 @@ int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, u
   a.types = types; a.keys = keys; a.key_lengths = klens; a.values = values;
   a.value_lengths_in = vlens; a.value_lengths_out = vlens; a.results = results;
   a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
-  return launch_batch<OP_MIXED, true>(t, a, (cudaStream_t)stream);
+  if (flags & MT_FLAG_SINGLE_PASS) return launch_batch<OP_MIXED, true>(t, a, (cudaStream_t)stream);
+  return launch_mixed_split(t, a, (cudaStream_t)stream);
 }
 
 int mt_scan(mt_masstree* t, const uint32_t* lower, const uint32_t* lower_lens, uint32_t maxK, uint32_t max_count,

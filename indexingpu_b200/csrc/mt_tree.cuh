@@ -35,9 +35,12 @@ constexpr uint32_t kLockSpins = 1u << 20;   // lock attempts before MT_ERR_LOCK_
 constexpr uint32_t kMaxRestarts = 1u << 14;
 
 #ifndef MT_CONC_LOAD
-#define MT_CONC_LOAD ::mtb::ld_order::ACQUIRE
+#define MT_CONC_LOAD ::mtb::ld_order::RELAXED
 #endif
-// Order of node loads in operations that run concurrently with writers.
+// Order of lock-free node loads in operations that run beside writers.
+// Relaxed gpu-scope loads are served by L2, the point of coherence, so a
+// pointer read from a published node leads to the already-published target;
+// the node checksum rejects any image that is torn or not yet written.
 constexpr ld_order kConc = MT_CONC_LOAD;
 // Suffix chains are immutable after publication; they are read after the
 // owning entry was read with kConc, from L2.
@@ -73,7 +76,7 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
       return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
-    __nanosleep(32u << (it < 5u ? it : 5u));
+    __nanosleep(32u << (it < 3u ? it : 3u));
   }
   if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT);
   return false;
@@ -554,6 +557,30 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
   return R_ERR;
 }
 
+// ---- lock-free presence check ------------------------------------------------------
+
+// Whether the key (its slice at `layer` is the border slice) is present in a
+// verified border image nd: returns 1 and the entry's value in *v if present,
+// 0 if absent.  A consistent image read without the lock is a valid
+// linearisation point for a miss, so update/erase/insert fail without locking.
+template <int T>
+MT_DEV int present_in_image(const tile<T>& t, const pool_view& p, const node<T>& nd, const uint32_t* key,
+                            uint32_t klen, uint32_t layer, uint32_t* v) {
+  const uint32_t slice = key[layer];
+  const bool more = layer + 1u < klen;
+  const int e = nd.match(t, slice, more);
+  if (e < 0) return 0;
+  const uint32_t st = ks_get(nd.ks, (uint32_t)e);
+  *v = nd.val_at(t, (uint32_t)e);
+  if (st != KS_SUFFIX) return 1;
+  if (!p.valid(*v)) return 1;  // let the locked path report it
+  suffix_head<T> h;
+  h.template load<kConcSuffix>(t, p, *v);
+  const uint32_t lk = klen - layer - 1u;
+  if (h.klen != lk) return 0;
+  return suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign == 0 ? 1 : 0;
+}
+
 // ---- update -------------------------------------------------------------------------
 
 template <int T>
@@ -574,6 +601,8 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
       const int e = nd.match(t, slice, true);
       if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
     }
+    uint32_t v0 = kInvalid;
+    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return R_FAIL;
     if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
     const int e = nd.match(t, slice, more);
     if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
@@ -582,12 +611,14 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
     if (st == KS_VALUE || st == KS_LONGVAL) return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
     if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
-    suffix_head<T> h;
-    h.template load<kConcSuffix>(t, p, v);
     const uint32_t lk = klen - layer - 1u;
-    if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
-      unlock_node(t, p, nd.idx);
-      return R_FAIL;
+    if (v != v0) {  // the chain changed since the lock-free check: compare again
+      suffix_head<T> h;
+      h.template load<kConcSuffix>(t, p, v);
+      if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
+        unlock_node(t, p, nd.idx);
+        return R_FAIL;
+      }
     }
     return replace_suffix(t, p, cache, nd, (uint32_t)e, v, key + layer + 1u, lk, val, vlen);
   }
@@ -610,13 +641,15 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
       const int e = nd.match(t, slice, true);
       if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
     }
+    uint32_t v0 = kInvalid;
+    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return R_FAIL;
     if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
     const int e = nd.match(t, slice, more);
     if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
     const uint32_t st = ks_get(nd.ks, (uint32_t)e);
     const uint32_t v = nd.val_at(t, (uint32_t)e);
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
-    if (st == KS_SUFFIX) {
+    if (st == KS_SUFFIX && v != v0) {
       if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);

@@ -26,7 +26,7 @@ import ctypes
 from . import _lib
 
 REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
-FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY = 1, 2, 4
+FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS = 1, 2, 4, 8
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG"}
 
@@ -93,6 +93,9 @@ class GpuMasstree:
     def set_tile_size(self, tile_size):
         self._check(self._lib.mt_set_tile_size(self._h, tile_size), "mt_set_tile_size")
 
+    def set_write_tile_size(self, tile_size):
+        self._check(self._lib.mt_set_write_tile_size(self._h, tile_size), "mt_set_write_tile_size")
+
     def set_blocks_per_sm(self, blocks_per_sm):
         self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
 
@@ -137,10 +140,10 @@ class GpuMasstree:
         self._check(rc, "mt_scan")
 
     def mixed_batch(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
-                    value_lengths, results, num_requests, stream=0):
+                    value_lengths, results, num_requests, stream=0, single_pass=False):
         rc = self._lib.mt_mixed_batch(self._h, _ptr(request_types), _ptr(keys), max_key_length, _ptr(key_lengths),
                                       _ptr(values), max_value_length, _ptr(value_lengths), _ptr(results),
-                                      num_requests, 0, _stream(stream))
+                                      num_requests, FLAG_SINGLE_PASS if single_pass else 0, _stream(stream))
         self._check(rc, "mt_mixed_batch")
 
     # -- status ---------------------------------------------------------------------
