@@ -37,7 +37,8 @@ enum {
   MT_ERR_INVALID_ARG = 4,
   MT_ERR_CUDA = 5,
   MT_ERR_RETRY_LIMIT = 6,  /* an insert restarted its descent too often */
-  MT_ERR_KEY_TOO_LONG = 7  /* scan depth beyond the scan frame capacity */
+  MT_ERR_KEY_TOO_LONG = 7, /* scan depth beyond the scan frame capacity */
+  MT_ERR_BATCH_TOO_LARGE = 8 /* batch larger than mt_mixed_batch_noalloc's fixed scratch */
 };
 
 /* Request kinds of mt_mixed_batch (reference macros.hpp:51-57). */
@@ -117,6 +118,28 @@ int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32
                    uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
                    uint32_t max_value_length, uint32_t* value_lengths, bool* results,
                    uint32_t num_requests, uint32_t flags, void* stream);
+
+/* mt_mixed_batch for callers that must not allocate device memory during the
+ * call: code that runs while a CUDA graph is being captured (cudaMalloc is not
+ * a stream operation and breaks the capture), request loops that must never
+ * wait on the driver's allocator, and programs that give the whole device
+ * budget to the slab pool.  mt_mixed_batch may cudaMalloc its partition scratch
+ * when a batch is larger than any before; this variant never calls cudaMalloc,
+ * cudaFree or any allocating routine.  Its scratch is one fixed array of
+ * 2 MiB + 128 B in the library, present on every GPU that loads it until the
+ * process exits, so num_requests is limited to 262144 (1 << 18); larger
+ * batches return MT_ERR_BATCH_TOO_LARGE and launch nothing.  Same arguments,
+ * results and error reporting as mt_mixed_batch.
+ * The first call on a device looks up the array's device address (once per
+ * device, with the tree's device current); make that first call before any
+ * stream capture.  All calls on one GPU share the array: calls whose work
+ * overlaps on the GPU (different streams, or different trees, without ordering
+ * between them) race on it and must be serialised by the caller.
+ * No counterpart in the reference. */
+int mt_mixed_batch_noalloc(mt_masstree* tree, const uint8_t* request_types, const uint32_t* keys,
+                           uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
+                           uint32_t max_value_length, uint32_t* value_lengths, bool* results,
+                           uint32_t num_requests, void* stream);
 
 /* Wait for `stream`, then return (and clear) the first device error recorded
  * since the previous mt_sync (MT_OK if none). */

@@ -24,6 +24,7 @@ SIGNATURES = {
     "mt_erase": (_int, [_p, _p, _u32, _p, _u32, _p, _u32, _p]),
     "mt_scan": (_int, [_p, _p, _p, _u32, _u32, _u32, _p, _p, _p, _p, _u32, _p, _p, _p, _u32, _p]),
     "mt_mixed_batch": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _u32, _p]),
+    "mt_mixed_batch_noalloc": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _p]),
     "mt_sync": (_int, [_p, _p]),
     "mt_stats": (_int, [_p, _p]),
     "mt_reclaim": (_int, [_p, _p]),

@@ -666,6 +666,7 @@ const char* mt_status_string(int s) {
     case MT_ERR_CUDA: return "CUDA error";
     case MT_ERR_RETRY_LIMIT: return "retry limit reached";
     case MT_ERR_KEY_TOO_LONG: return "key deeper than scan frame capacity";
+    case MT_ERR_BATCH_TOO_LARGE: return "batch larger than the fixed no-allocation scratch";
     default: return "unknown status";
   }
 }
@@ -816,4 +817,80 @@ extern "C" int mt_selftest_line_atomicity(uint32_t tile_size, uint32_t nlines, u
   *reads = hctr[0];
   *torn = hctr[1];
   return MT_OK;
+}
+
+// ---- mixed batch that allocates nothing -------------------------------------------
+//
+// mt_mixed_batch keeps its partition scratch in memory it allocates with
+// cudaMalloc the first time a batch is larger than any before.  Some callers
+// cannot allocate at that point: code running while a CUDA graph is being
+// captured (cudaMalloc is not a stream operation and breaks the capture),
+// latency-critical request loops that must never take the driver's allocation
+// lock, and hosts that hand the whole device budget to the slab pool up front.
+// mt_mixed_batch_noalloc serves them: its partition scratch is the fixed
+// file-scope array below, sized for kNoAllocMaxRequests requests (2 MiB plus
+// one line, held on every GPU that loads this library until the process exits).
+
+namespace {
+constexpr uint32_t kNoAllocMaxRequests = 1u << 18;
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+// [0, 32): find / write counters (one line); then find indices, write indices.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[32u + 2u * kNoAllocMaxRequests];
+
+namespace {
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device with that device current and kept.
+int noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return MT_ERR_CUDA;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return MT_ERR_CUDA;
+    g_noalloc_addr[dev] = static_cast<uint32_t*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return MT_OK;
+}
+}  // namespace
+
+extern "C" int mt_mixed_batch_noalloc(mt_masstree* t, const uint8_t* types, const uint32_t* keys, uint32_t maxK,
+                                      const uint32_t* klens, uint32_t* values, uint32_t maxV, uint32_t* vlens,
+                                      bool* results, uint32_t n, void* stream) {
+  if (!t || (n && (!types || !keys || !values || !vlens || maxK == 0 || maxV == 0))) return MT_ERR_INVALID_ARG;
+  if (n > kNoAllocMaxRequests) return MT_ERR_BATCH_TOO_LARGE;
+  if (n == 0) return MT_OK;
+  uint32_t* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  batch_args a{};
+  a.types = types; a.keys = keys; a.key_lengths = klens; a.values = values;
+  a.value_lengths_in = vlens; a.value_lengths_out = vlens; a.results = results;
+  a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
+  rc = launch_reclaim(t, s);
+  if (rc) return rc;
+  uint32_t* counts = scratch;
+  uint32_t* find_idx = scratch + 32;
+  uint32_t* write_idx = find_idx + n;
+  // The array keeps the previous call's contents: the counters must restart at 0.
+  if (cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+  partition_kernel<<<std::max(1, std::min(t->sms * 8, (int)((n + 255) / 256))), 256, 0, s>>>(types, n, find_idx,
+                                                                                             write_idx, counts);
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
+  batch_args f = a;
+  f.index = find_idx;
+  f.n_dev = counts;
+  rc = launch_batch_tile<OP_MIXED, true>(t, t->tile_size, f, s);
+  if (rc) return rc;
+  batch_args w = a;
+  w.index = write_idx;
+  w.n_dev = counts + 1;
+  return launch_batch_tile<OP_MIXED, true>(t, t->write_tile_size, w, s);
 }

@@ -28,7 +28,7 @@ from . import _lib
 REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
 FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS = 1, 2, 4, 8
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
-          5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG"}
+          5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
 
 class MasstreeError(RuntimeError):
