@@ -30,7 +30,21 @@ constexpr int kBlock = 128;
 constexpr uint32_t kShards = 64;
 constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
 
-enum op_kind : int { OP_FIND = 0, OP_INSERT = 1, OP_UPSERT = 2, OP_UPDATE = 3, OP_ERASE = 4, OP_MIXED = 5 };
+#ifndef MT_MIN_BLOCKS_PER_SM
+#define MT_MIN_BLOCKS_PER_SM 1  // occupancy hint for the batch kernels (caps registers)
+#endif
+
+// Kernel flavours.  OP_PASS_* serve one class of a partitioned mixed batch and
+// compile only that class's code (smaller kernels, fewer instruction-cache
+// misses than OP_MIXED, which handles every kind).
+enum op_kind : int {
+  OP_FIND = 0, OP_INSERT = 1, OP_UPSERT = 2, OP_UPDATE = 3, OP_ERASE = 4, OP_MIXED = 5,
+  OP_PASS_INSERT = 6, OP_PASS_UPDERASE = 7
+};
+template <int OP> constexpr bool op_finds = OP == OP_FIND || OP == OP_MIXED;
+template <int OP> constexpr bool op_inserts = OP == OP_INSERT || OP == OP_UPSERT || OP == OP_MIXED || OP == OP_PASS_INSERT;
+template <int OP> constexpr bool op_updates = OP == OP_UPDATE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
+template <int OP> constexpr bool op_erases = OP == OP_ERASE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
 
 struct batch_args {
   const uint8_t* types;
@@ -74,6 +88,35 @@ __global__ void partition_kernel(const uint8_t* types, uint32_t n, uint32_t* fin
   }
 }
 
+// Split a mixed batch into finds, inserts and updates+erases (one atomic per
+// warp and class).  counts = {finds, inserts, updates+erases}.
+__global__ void partition3_kernel(const uint8_t* types, uint32_t n, uint32_t* find_idx, uint32_t* insert_idx,
+                                  uint32_t* upderase_idx, uint32_t* counts) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    const uint32_t k = i < n ? types[i] : 0xFFu;
+    const uint32_t m[3] = {__ballot_sync(0xFFFFFFFFu, k == MT_REQ_FIND),
+                           __ballot_sync(0xFFFFFFFFu, k == MT_REQ_INSERT),
+                           __ballot_sync(0xFFFFFFFFu, i < n && k != MT_REQ_FIND && k != MT_REQ_INSERT)};
+    uint32_t b[3] = {0, 0, 0};
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (m[c]) b[c] = atomicAdd(counts + c, (uint32_t)__popc(m[c]));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[c] = __shfl_sync(0xFFFFFFFFu, b[c], 0);
+    const uint32_t below = (1u << lane) - 1u;
+    if (i < n) {
+      const int c = k == MT_REQ_FIND ? 0 : (k == MT_REQ_INSERT ? 1 : 2);
+      uint32_t* dst = c == 0 ? find_idx : (c == 1 ? insert_idx : upderase_idx);
+      dst[b[c] + __popc(m[c] & below)] = i;
+    }
+  }
+}
+
 struct scan_args {
   const uint32_t* lower;
   const uint32_t* lower_lengths;
@@ -97,25 +140,36 @@ template <int T, int OP, bool CONC>
 MT_DEV void run_request(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const batch_args& a,
                         uint32_t j, uint32_t kind, uint32_t klen, uint32_t vlen, uint32_t& res, uint32_t& vout) {
   const uint32_t* key = a.keys + (size_t)j * a.max_key_length;
-  if (kind == MT_REQ_FIND) {
-    uint32_t* out = a.values ? a.values + (size_t)j * a.max_value_length : nullptr;
-    const uint32_t l = coop_find<T, CONC>(t, tv, key, klen, out, a.max_value_length);
-    vout = l;
-  } else if (kind == MT_REQ_INSERT) {
-    const uint32_t* val = a.values + (size_t)j * a.max_value_length;
-    const int r = (OP == OP_UPSERT) ? coop_insert<T, true>(t, tv, cache, key, klen, val, vlen)
-                                    : coop_insert<T, false>(t, tv, cache, key, klen, val, vlen);
-    res = (r == R_OK) ? 1u : 0u;
-  } else if (kind == MT_REQ_UPDATE) {
-    const uint32_t* val = a.values + (size_t)j * a.max_value_length;
-    res = (coop_update<T>(t, tv, cache, key, klen, val, vlen) == R_OK) ? 1u : 0u;
-  } else {
-    res = (coop_erase<T>(t, tv, key, klen) == R_OK) ? 1u : 0u;
+  if constexpr (op_finds<OP>) {
+    if (kind == MT_REQ_FIND) {
+      uint32_t* out = a.values ? a.values + (size_t)j * a.max_value_length : nullptr;
+      vout = coop_find<T, CONC>(t, tv, key, klen, out, a.max_value_length);
+      return;
+    }
+  }
+  if constexpr (op_inserts<OP>) {
+    if (kind == MT_REQ_INSERT) {
+      const uint32_t* val = a.values + (size_t)j * a.max_value_length;
+      const int r = (OP == OP_UPSERT) ? coop_insert<T, true>(t, tv, cache, key, klen, val, vlen)
+                                      : coop_insert<T, false>(t, tv, cache, key, klen, val, vlen);
+      res = (r == R_OK) ? 1u : 0u;
+      return;
+    }
+  }
+  if constexpr (op_updates<OP>) {
+    if (kind == MT_REQ_UPDATE) {
+      const uint32_t* val = a.values + (size_t)j * a.max_value_length;
+      res = (coop_update<T>(t, tv, cache, key, klen, val, vlen) == R_OK) ? 1u : 0u;
+      return;
+    }
+  }
+  if constexpr (op_erases<OP>) {
+    if (kind == MT_REQ_ERASE) res = (coop_erase<T>(t, tv, key, klen) == R_OK) ? 1u : 0u;
   }
 }
 
 template <int T, int OP, bool CONC>
-__global__ void __launch_bounds__(kBlock) batch_kernel(tree_view tv, batch_args a) {
+__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batch_kernel(tree_view tv, batch_args a) {
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
@@ -131,9 +185,9 @@ __global__ void __launch_bounds__(kBlock) batch_kernel(tree_view tv, batch_args 
     const uint32_t i = (valid && a.index) ? a.index[pos] : pos;
     uint32_t kind = 0, klen = 0, vlen = 0;
     if (valid) {
-      if constexpr (OP == OP_MIXED) kind = a.types[i];
+      if constexpr (OP == OP_MIXED || OP == OP_PASS_UPDERASE) kind = a.types[i];
       else if constexpr (OP == OP_FIND) kind = MT_REQ_FIND;
-      else if constexpr (OP == OP_INSERT || OP == OP_UPSERT) kind = MT_REQ_INSERT;
+      else if constexpr (OP == OP_INSERT || OP == OP_UPSERT || OP == OP_PASS_INSERT) kind = MT_REQ_INSERT;
       else if constexpr (OP == OP_UPDATE) kind = MT_REQ_UPDATE;
       else kind = MT_REQ_ERASE;
       klen = a.key_lengths ? a.key_lengths[i] : a.max_key_length;
@@ -365,17 +419,18 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   if (t->split_idx) cudaFree(t->split_idx);
   t->split_idx = nullptr;
   t->split_cap = 0;
-  // [counts(32 words, one line)] [find indices n] [write indices n]
-  if (cudaMalloc(&t->split_idx, (32u + 2ull * n) * sizeof(uint32_t)) != cudaSuccess) return MT_ERR_OOM;
+  // [counts(32 words, one line)] [find indices n] [insert indices n] [update/erase indices n]
+  if (cudaMalloc(&t->split_idx, (32u + 3ull * n) * sizeof(uint32_t)) != cudaSuccess) return MT_ERR_OOM;
   t->split_cap = n;
   return MT_OK;
 }
 
-// A mixed batch as three launches: partition by kind, then every find with the
-// find tile width, then every write (insert/update/erase) with the write tile
-// width.  Finds and writes of one batch have no defined order, so serving the
-// finds first is one of the orders the reference allows; it removes the
-// find/write divergence between the tiles of a warp.
+// A mixed batch as four launches: partition by kind, then every find with the
+// find tile width, then the inserts, then the updates and erases, both with the
+// write tile width.  Requests of one mixed batch have no defined order, so
+// serving them class by class is one of the orders the reference allows; it
+// removes the divergence between the tiles of a warp and keeps each kernel's
+// code small.
 int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   if (a.n == 0) return MT_OK;
   int rc = ensure_split_scratch(t, a.n, s);
@@ -384,20 +439,25 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   if (rc) return rc;
   uint32_t* counts = t->split_idx;
   uint32_t* find_idx = t->split_idx + 32;
-  uint32_t* write_idx = find_idx + a.n;
-  if (cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
-  partition_kernel<<<std::max(1, std::min(t->sms * 8, (int)((a.n + 255) / 256))), 256, 0, s>>>(
-      a.types, a.n, find_idx, write_idx, counts);
+  uint32_t* insert_idx = find_idx + a.n;
+  uint32_t* upderase_idx = insert_idx + a.n;
+  if (cudaMemsetAsync(counts, 0, 3 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+  partition3_kernel<<<std::max(1, std::min(t->sms * 8, (int)((a.n + 255) / 256))), 256, 0, s>>>(
+      a.types, a.n, find_idx, insert_idx, upderase_idx, counts);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
   batch_args f = a;
   f.index = find_idx;
   f.n_dev = counts;
-  rc = launch_batch_tile<OP_MIXED, true>(t, t->tile_size, f, s);
+  rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, s);
   if (rc) return rc;
   batch_args w = a;
-  w.index = write_idx;
+  w.index = insert_idx;
   w.n_dev = counts + 1;
-  return launch_batch_tile<OP_MIXED, true>(t, t->write_tile_size, w, s);
+  rc = launch_batch_tile<OP_PASS_INSERT, true>(t, t->write_tile_size, w, s);
+  if (rc) return rc;
+  w.index = upderase_idx;
+  w.n_dev = counts + 2;
+  return launch_batch_tile<OP_PASS_UPDERASE, true>(t, t->write_tile_size, w, s);
 }
 
 template <int T, bool CONC>

@@ -176,6 +176,114 @@ MT_DEV uint32_t split_pos(const tile<T>& t, const node<T>& nd) {
   return p;
 }
 
+// Split the full node nd, locked by the caller (with its parent `parent` when
+// nd is not a layer root).  Returns 0 with nd = the half covering `slice`
+// (locked iff it is a border node) and parent updated; 1 when the parent
+// changed and the layer must be descended again; -1 on error.  Nothing else is
+// left locked.  (Kept inline: ptxas 12.9 crashes on an out-of-line version.)
+template <int T>
+MT_DEV int split_full(const tile<T>& t, const pool_view& p, slab_cache<T>& cache, uint32_t slice,
+                                       node<T>& nd, uint32_t& parent, uint32_t& restarts) {
+  const uint32_t idx = nd.idx;
+  const uint32_t sp = split_pos(t, nd);
+  const uint32_t left_high = nd.key_at(t, sp - 1);
+  const bool go_right = slice > left_high;
+  const bool border = nd.is_border();
+  node<T> rn;
+  if (nd.is_root()) {
+    // The layer root keeps its slab: its entries move to two new children.
+    const uint32_t L = cache.allocate(t, p);
+    const uint32_t R = (L != kInvalid) ? cache.allocate(t, p) : kInvalid;
+    if (R == kInvalid) {
+      if (L != kInvalid && t.leader()) retire_slab(p, L);
+      unlock_node(t, p, idx);
+      return -1;
+    }
+    node<T> ln;
+    rn.take_upper_from(t, nd, sp);
+    rn.idx = R;
+    rn.meta = (border ? META_BORDER : 0u) | (nd.count() - sp);
+    rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
+    rn.high = nd.high;
+    rn.sib = kInvalid;
+#pragma unroll
+    for (int k = 0; k < node<T>::W; ++k) ln.w[k] = nd.w[k];
+    ln.truncate(t, sp);
+    ln.idx = L;
+    ln.meta = (border ? META_BORDER : 0u) | META_SIB | sp;
+    ln.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
+    ln.high = left_high;
+    ln.sib = R;
+    // The child we continue into stays locked if it is a border node.
+    if (go_right && border) rn.meta |= META_LOCK;
+    if (!go_right && border) ln.meta |= META_LOCK;
+    publish_new(t, p, rn);
+    publish_new(t, p, ln);
+    const uint32_t old_high = nd.high;
+    nd.clear_words();
+    nd.set_word(t, 0, left_high);
+    nd.set_word(t, 1, L);
+    nd.set_word(t, 2, old_high);
+    nd.set_word(t, 3, R);
+    nd.meta = (nd.meta & ~(META_COUNT | META_BORDER)) | 2u;
+    nd.ks = 0u;
+    publish_unlock(t, p, nd);
+    parent = idx;
+    if (go_right) {
+      nd = rn;
+    } else {
+      nd = ln;
+    }
+  } else {
+    if (parent == kInvalid || ++restarts > kMaxRestarts) {
+      unlock_node(t, p, idx);
+      if (restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+      return 1;
+    }
+    node<T> pn;
+    if (!lock_load(t, p, parent, pn)) { unlock_node(t, p, idx); return -1; }
+    const int j = pn.is_border() ? -1 : pn.child_slot_of(t, idx);
+    if (pn.full() || j < 0) {
+      // The parent changed under us: start the layer again.
+      unlock_node(t, p, parent);
+      unlock_node(t, p, idx);
+      if (++restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+      return 1;
+    }
+    const uint32_t R = cache.allocate(t, p);
+    if (R == kInvalid) {
+      unlock_node(t, p, parent);
+      unlock_node(t, p, idx);
+      return -1;
+    }
+    rn.take_upper_from(t, nd, sp);
+    rn.idx = R;
+    rn.meta = (border ? META_BORDER : 0u) | (nd.meta & META_SIB) | (nd.count() - sp);
+    rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
+    rn.high = nd.high;
+    rn.sib = nd.sib;
+    if (go_right && border) rn.meta |= META_LOCK;
+    nd.truncate(t, sp);
+    nd.meta = (nd.meta & ~META_COUNT) | META_SIB | sp;
+    nd.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
+    nd.high = left_high;
+    nd.sib = R;
+    // Parent: (left_high -> idx) inserted at j; old entry j (-> idx) now -> R.
+    pn.insert_at(t, (uint32_t)j, left_high, idx, 0u);
+    pn.set_entry(t, (uint32_t)j + 1u, R, 0u);
+    // Write order: right, left, parent.
+    publish_new(t, p, rn);
+    publish_locked(t, p, nd);
+    publish_unlock(t, p, pn);
+    if (go_right) {
+      unlock_node(t, p, idx);
+      nd = rn;
+    }
+    parent = pn.idx;  // both halves hang under pn
+  }
+  return 0;
+}
+
 // Descent of one layer for an insert, splitting full nodes on the way.
 // Returns 0 with nd = the LOCKED, non-full border node covering `slice`;
 // 1 when the border node already holds a LINK for (slice, continues) (link set,
@@ -217,106 +325,9 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
       continue;
     }
     // nd is full and locked: split it.
-    const uint32_t sp = split_pos(t, nd);
-    const uint32_t left_high = nd.key_at(t, sp - 1);
-    const bool go_right = slice > left_high;
-    const bool border = nd.is_border();
-    node<T> rn;
-    if (nd.is_root()) {
-      // The layer root keeps its slab: its entries move to two new children.
-      const uint32_t L = cache.allocate(t, p);
-      const uint32_t R = (L != kInvalid) ? cache.allocate(t, p) : kInvalid;
-      if (R == kInvalid) {
-        if (L != kInvalid && t.leader()) retire_slab(p, L);
-        unlock_node(t, p, idx);
-        return -1;
-      }
-      node<T> ln;
-      rn.take_upper_from(t, nd, sp);
-      rn.idx = R;
-      rn.meta = (border ? META_BORDER : 0u) | (nd.count() - sp);
-      rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
-      rn.high = nd.high;
-      rn.sib = kInvalid;
-#pragma unroll
-      for (int k = 0; k < node<T>::W; ++k) ln.w[k] = nd.w[k];
-      ln.truncate(t, sp);
-      ln.idx = L;
-      ln.meta = (border ? META_BORDER : 0u) | META_SIB | sp;
-      ln.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
-      ln.high = left_high;
-      ln.sib = R;
-      // The child we continue into stays locked if it is a border node.
-      if (go_right && border) rn.meta |= META_LOCK;
-      if (!go_right && border) ln.meta |= META_LOCK;
-      publish_new(t, p, rn);
-      publish_new(t, p, ln);
-      const uint32_t old_high = nd.high;
-      nd.clear_words();
-      nd.set_word(t, 0, left_high);
-      nd.set_word(t, 1, L);
-      nd.set_word(t, 2, old_high);
-      nd.set_word(t, 3, R);
-      nd.meta = (nd.meta & ~(META_COUNT | META_BORDER)) | 2u;
-      nd.ks = 0u;
-      publish_unlock(t, p, nd);
-      parent = idx;
-      if (go_right) {
-        nd = rn;
-      } else {
-        nd = ln;
-      }
-    } else {
-      if (parent == kInvalid || ++restarts > kMaxRestarts) {
-        unlock_node(t, p, idx);
-        if (restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
-        idx = root;
-        parent = kInvalid;
-        continue;
-      }
-      node<T> pn;
-      if (!lock_load(t, p, parent, pn)) { unlock_node(t, p, idx); return -1; }
-      const int j = pn.is_border() ? -1 : pn.child_slot_of(t, idx);
-      if (pn.full() || j < 0) {
-        // The parent changed under us: start the layer again.
-        unlock_node(t, p, parent);
-        unlock_node(t, p, idx);
-        if (++restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
-        idx = root;
-        parent = kInvalid;
-        continue;
-      }
-      const uint32_t R = cache.allocate(t, p);
-      if (R == kInvalid) {
-        unlock_node(t, p, parent);
-        unlock_node(t, p, idx);
-        return -1;
-      }
-      rn.take_upper_from(t, nd, sp);
-      rn.idx = R;
-      rn.meta = (border ? META_BORDER : 0u) | (nd.meta & META_SIB) | (nd.count() - sp);
-      rn.ks = border ? (nd.ks >> (2u * sp)) : 0u;
-      rn.high = nd.high;
-      rn.sib = nd.sib;
-      if (go_right && border) rn.meta |= META_LOCK;
-      nd.truncate(t, sp);
-      nd.meta = (nd.meta & ~META_COUNT) | META_SIB | sp;
-      nd.ks = border ? (nd.ks & ((1u << (2u * sp)) - 1u)) : 0u;
-      nd.high = left_high;
-      nd.sib = R;
-      // Parent: (left_high -> idx) inserted at j; old entry j (-> idx) now -> R.
-      pn.insert_at(t, (uint32_t)j, left_high, idx, 0u);
-      pn.set_entry(t, (uint32_t)j + 1u, R, 0u);
-      // Write order: right, left, parent.
-      publish_new(t, p, rn);
-      publish_locked(t, p, nd);
-      publish_unlock(t, p, pn);
-      if (go_right) {
-        unlock_node(t, p, idx);
-        nd = rn;
-      }
-      parent = pn.idx;  // both halves hang under pn
-    }
+    const int sr = split_full(t, p, cache, slice, nd, parent, restarts);
+    if (sr < 0) return -1;
+    if (sr == 1) { idx = root; parent = kInvalid; continue; }
     // nd is now the non-full half covering slice; locked iff border.
     if (nd.is_border()) {
       nd.meta |= META_LOCK;
