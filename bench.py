@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--preload", type=int, default=1 << 24)
     ap.add_argument("--batch", type=int, default=1 << 20)
-    ap.add_argument("--tile", type=int, default=16, help="lanes per find")
+    ap.add_argument("--tile", type=int, default=8, help="lanes per find")
     ap.add_argument("--write-tile", type=int, default=32, help="lanes per insert/update/erase")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=16)

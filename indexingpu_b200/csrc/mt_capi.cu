@@ -31,7 +31,7 @@ constexpr uint32_t kShards = 64;
 constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
 
 #ifndef MT_MIN_BLOCKS_PER_SM
-#define MT_MIN_BLOCKS_PER_SM 1  // occupancy hint for the batch kernels (caps registers)
+#define MT_MIN_BLOCKS_PER_SM 8  // occupancy hint for the batch kernels: caps registers at 64
 #endif
 
 // Kernel flavours.  OP_PASS_* serve one class of a partitioned mixed batch and

@@ -31,7 +31,7 @@
 namespace mtb {
 
 constexpr uint32_t kMaxHops = 1u << 16;     // node visits per operation
-constexpr uint32_t kLockSpins = 1u << 20;   // lock attempts before MT_ERR_LOCK_TIMEOUT
+constexpr uint32_t kLockSpins = 1u << 18;   // lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
 constexpr uint32_t kMaxRestarts = 1u << 14;
 
 #ifndef MT_CONC_LOAD
@@ -62,12 +62,20 @@ MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
   t.sync();
 }
 
+// Test-and-test-and-set: waiters poll the meta word with plain loads and only
+// try the atomic when it reads unlocked, with jittered exponential backoff
+// (64 ns .. 4 us), so a hot node's holder is not slowed by a storm of atomics
+// on its line.
 template <int T>
 MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T>& nd) {
   uint32_t* mw = p.addr(idx) + WORD_META;
+  uint32_t backoff = 64u;
+  uint32_t jitter = (idx * 0x9E3779B1u) ^ (uint32_t)clock();
   for (uint32_t it = 0; it < kLockSpins; ++it) {
-    uint32_t old = 0;
-    if (t.leader()) old = atom_or_acquire(mw, META_LOCK);
+    uint32_t old = META_LOCK;
+    if (t.leader()) {
+      if (!(ld_relaxed_u32(mw) & META_LOCK)) old = atom_or_acquire(mw, META_LOCK);
+    }
     old = t.shfl(old, 0);
     if (!(old & META_LOCK)) {
       t.sync();
@@ -76,7 +84,9 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
       return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
-    __nanosleep(32u << (it < 3u ? it : 3u));
+    jitter = jitter * 1664525u + 1013904223u;
+    __nanosleep(backoff + ((jitter >> 16) & (backoff - 1u)));
+    if (backoff < 2048u) backoff <<= 1;
   }
   if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT);
   return false;
