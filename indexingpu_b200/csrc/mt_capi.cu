@@ -738,17 +738,29 @@ const char* mt_status_string(int s) {
 namespace {
 
 struct validator {
-  const std::vector<uint32_t>& img;  // slab words
-  uint32_t nslabs;
+  // Used prefix of every shard (slabs past a shard's bump pointer were never
+  // handed out).
+  std::vector<std::vector<uint32_t>> img;
+  std::vector<uint32_t> used;
+  uint32_t shard_slabs = 1;
+  std::vector<bool> seen;  // slab reached from the root (each at most once)
   uint64_t keys = 0, nodes = 0, chains = 0;
   std::string err;
   int depth_limit = 1 << 16;
 
-  const uint32_t* slab(uint32_t i) const { return img.data() + (size_t)i * 32u; }
-  bool ok(uint32_t i) { return i < nslabs; }
+  bool ok(uint32_t i) const {
+    const uint32_t s = i / shard_slabs;
+    return s < used.size() && (i % shard_slabs) < used[s];
+  }
+  const uint32_t* slab(uint32_t i) const { return img[i / shard_slabs].data() + (size_t)(i % shard_slabs) * 32u; }
   bool fail(const std::string& m) {
     if (err.empty()) err = m;
     return false;
+  }
+  bool mark(uint32_t i) {
+    if (seen[i]) return fail("slab reachable twice (handed out twice)");
+    seen[i] = true;
+    return true;
   }
 
   bool chain(uint32_t head) {
@@ -757,9 +769,11 @@ struct validator {
     const uint32_t kl = hdr & kMaxLen16, vl = hdr >> 16;
     const uint32_t need = suf_nodes(kl, vl);
     uint32_t c = head;
+    if (!mark(c)) return false;
     for (uint32_t n = 1; n < need; ++n) {
       c = slab(c)[SUF_WORD_NEXT];
       if (!ok(c)) return fail("suffix chain shorter than its header");
+      if (!mark(c)) return false;
     }
     if (slab(c)[SUF_WORD_NEXT] != kInvalid) return fail("suffix chain longer than its header");
     ++chains;
@@ -769,6 +783,7 @@ struct validator {
   // Validate the subtree at idx covering (lo, hi] (lo exclusive unless first).
   bool subtree(uint32_t idx, uint64_t lo_excl, uint32_t hi, int level, int& border_level, int layer_depth) {
     if (!ok(idx)) return fail("node index out of range");
+    if (!mark(idx)) return false;
     const uint32_t* w = slab(idx);
     const uint32_t meta = w[WORD_META], ks = w[WORD_KS], n = meta & META_COUNT;
     ++nodes;
@@ -828,23 +843,51 @@ extern "C" int mt_validate(mt_masstree* t, uint64_t* num_keys, char* msg, size_t
   if (!t) return MT_ERR_INVALID_ARG;
   if (cudaDeviceSynchronize() != cudaSuccess) return MT_ERR_CUDA;
   const pool_view& p = t->tv.pool;
-  std::vector<uint32_t> img((size_t)p.num_slabs * 32u, 0u);
   const size_t nctr = (size_t)p.num_shards * 3u * kCtrStride;
   std::vector<int> h(nctr);
   if (cudaMemcpy(h.data(), p.ctr, nctr * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_CUDA;
+  validator v;
+  v.shard_slabs = p.shard_slabs;
+  v.img.resize(p.num_shards);
+  v.used.resize(p.num_shards);
+  v.seen.assign(p.num_slabs, false);
+  std::vector<uint32_t> freed;  // free-stack and limbo entries
   for (uint32_t s = 0; s < p.num_shards; ++s) {
     const int bump = std::min<int>(std::max(h[(3 * s + 1) * kCtrStride], 0), (int)p.shard_slabs);
-    if (bump == 0) continue;
-    const size_t off = (size_t)s * p.shard_slabs * 32u;
-    if (cudaMemcpy(img.data() + off, p.slabs + off, (size_t)bump * 128u, cudaMemcpyDeviceToHost) != cudaSuccess)
+    v.used[s] = (uint32_t)bump;
+    if (bump > 0) {
+      v.img[s].resize((size_t)bump * 32u);
+      const size_t off = (size_t)s * p.shard_slabs * 32u;
+      if (cudaMemcpy(v.img[s].data(), p.slabs + off, (size_t)bump * 128u, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MT_ERR_CUDA;
+    }
+    const int top = std::max(h[(3 * s + 0) * kCtrStride], 0);
+    const int lim = std::max(h[(3 * s + 2) * kCtrStride], 0);
+    const size_t base = freed.size();
+    freed.resize(base + top + lim);
+    if (top > 0 && cudaMemcpy(freed.data() + base, p.free_stack + (size_t)s * p.shard_slabs, (size_t)top * 4u,
+                              cudaMemcpyDeviceToHost) != cudaSuccess)
+      return MT_ERR_CUDA;
+    if (lim > 0 && cudaMemcpy(freed.data() + base + top, p.limbo + (size_t)s * p.shard_slabs, (size_t)lim * 4u,
+                              cudaMemcpyDeviceToHost) != cudaSuccess)
       return MT_ERR_CUDA;
   }
-  validator v{img, p.num_slabs};
-  const bool good = v.layer(t->tv.root, 0);
+  bool good = v.layer(t->tv.root, 0);
+  // Allocator invariant: a free or retired slab is neither reachable nor listed twice.
+  if (good) {
+    std::vector<bool> listed(p.num_slabs, false);
+    for (uint32_t f : freed) {
+      if (f >= p.num_slabs) { good = v.fail("free list holds an out-of-range slab"); break; }
+      if (v.seen[f]) { good = v.fail("reachable slab is on a free list"); break; }
+      if (listed[f]) { good = v.fail("slab listed twice on the free lists"); break; }
+      listed[f] = true;
+    }
+  }
   if (num_keys) *num_keys = v.keys;
   if (msg && msg_len) {
-    std::snprintf(msg, msg_len, "%s (keys %llu, nodes %llu, chains %llu)", good ? "ok" : v.err.c_str(),
-                  (unsigned long long)v.keys, (unsigned long long)v.nodes, (unsigned long long)v.chains);
+    std::snprintf(msg, msg_len, "%s (keys %llu, nodes %llu, chains %llu, free+limbo %zu)",
+                  good ? "ok" : v.err.c_str(), (unsigned long long)v.keys, (unsigned long long)v.nodes,
+                  (unsigned long long)v.chains, freed.size());
   }
   return good ? MT_OK : MT_ERR_CORRUPT;
 }

@@ -221,13 +221,19 @@ MT_DEV uint32_t suffix_get_value(const tile<T>& t, const pool_view& p, const suf
 // Retire every slab of a chain (leader lane walks the links).
 template <int T, ld_order O>
 MT_DEV void suffix_retire(const tile<T>& t, const pool_view& p, uint32_t head) {
-  if (t.leader()) {
+  if (t.leader() && p.valid(head)) {
+    // Walk exactly the slabs the header accounts for, so that a damaged link
+    // can never free slabs that belong to something else.
+    const uint32_t hdr = ld_word<O>(p.addr(head) + SUF_WORD_HDR);
+    const uint32_t nn = suf_nodes(hdr & kMaxLen16, hdr >> 16);
     uint32_t c = head;
-    for (uint32_t guard = 0; guard < (1u << 16) && p.valid(c); ++guard) {
+    for (uint32_t q = 0; q < nn; ++q) {
+      if (!p.valid(c)) { record_error(p, ERR_CORRUPT); break; }
       const uint32_t nx = ld_word<O>(p.addr(c) + SUF_WORD_NEXT);
       retire_slab(p, c);
       c = nx;
     }
+    if (c != kInvalid) record_error(p, ERR_CORRUPT);
   }
   t.sync();
 }
