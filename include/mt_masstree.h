@@ -50,6 +50,21 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
 #define MT_FLAG_USE_UPPER_KEY 4u    /* scan stops after upper_keys (reference `use_upper_key`) */
 #define MT_FLAG_SINGLE_PASS 8u      /* mixed_batch: one kernel for every kind instead of
                                        finds-then-writes passes (comparison switch) */
+#define MT_FLAG_BUCKET_KEYS 16u     /* mixed_batches: serve short keys before long keys in
+                                       every request class */
+
+/* One sub-batch of mt_mixed_batches: the buffers of one mt_mixed_batch call
+ * (device pointers; max lengths are common to all sub-batches). */
+typedef struct mt_subbatch {
+  const uint8_t* request_types;
+  const uint32_t* keys;
+  const uint32_t* key_lengths; /* may be NULL */
+  uint32_t* values;
+  uint32_t* value_lengths;
+  bool* results;               /* may be NULL */
+  uint32_t num_requests;
+  uint32_t reserved;
+} mt_subbatch;
 
 typedef struct mt_stats_t {
   uint64_t total_slabs;     /* slabs in the pool (128 bytes each) */
@@ -118,6 +133,23 @@ int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32
                    uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
                    uint32_t max_value_length, uint32_t* value_lengths, bool* results,
                    uint32_t num_requests, uint32_t flags, void* stream);
+
+/* Size the scratch of mt_mixed_batches for up to max_subbatches sub-batches
+ * and max_total_requests requests in one call (allocates; call it before any
+ * graph capture).  New in this library. */
+int mt_batches_reserve(mt_masstree* tree, uint32_t max_subbatches, uint64_t max_total_requests);
+
+/* Serve num_subbatches mixed batches in order, with the results of one
+ * mt_mixed_batch call per sub-batch, in one persistent cooperative launch
+ * (plus a partition pass): sub-batch k+1 sees every effect of sub-batch k.
+ * `subbatches` is a DEVICE array of descriptors; nothing is read back to the
+ * host, so the call can be captured in a CUDA graph and replayed after the
+ * descriptors' contents change.  Needs mt_batches_reserve; flags may hold
+ * MT_FLAG_BUCKET_KEYS.  Find tile width: mt_set_tile_size (4/8/16/32); write
+ * tile width: mt_set_write_tile_size (16 or 32).  The batched counterpart of
+ * the reference's per-call mixed_batch (gpu_masstree.hpp:173-191). */
+int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t num_subbatches,
+                     uint32_t max_key_length, uint32_t max_value_length, uint32_t flags, void* stream);
 
 /* mt_mixed_batch for callers that must not allocate device memory during the
  * call: code that runs while a CUDA graph is being captured (cudaMalloc is not

@@ -11,13 +11,13 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libmt_b200.so")
-SOURCES = ["mt_capi.cu"]
-HEADERS = ["mt_tile.cuh", "mt_pool.cuh", "mt_node.cuh", "mt_suffix.cuh", "mt_tree.cuh"]
+SOURCES = ["mt_capi.cu", "mt_batches.cu"]
+HEADERS = ["mt_tile.cuh", "mt_pool.cuh", "mt_node.cuh", "mt_suffix.cuh", "mt_tree.cuh", "mt_internal.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -33,10 +33,22 @@ def build(force=False, verbose=True, extra_flags=()):
     deps.append(os.path.join(ROOT, "include", "mt_masstree.h"))
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = ["nvcc", *NVCC_FLAGS, *extra_flags, *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
+    # One object per translation unit, compiled in parallel, then linked.
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        cmd = ["nvcc", *NVCC_FLAGS, *extra_flags, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    for pr in procs:
+        if pr.wait() != 0:
+            raise subprocess.CalledProcessError(pr.returncode, "nvcc")
+    link = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB + ".tmp"]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.check_call(cmd)
+        print(" ".join(link), flush=True)
+    subprocess.check_call(link)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -21,45 +21,9 @@
 #include <unordered_map>
 #include <vector>
 
-#include "mt_tree.cuh"
-#include "../../include/mt_masstree.h"
+#include "mt_internal.cuh"
 
 namespace mtb {
-
-constexpr int kBlock = 128;
-constexpr uint32_t kShards = 64;
-constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
-
-#ifndef MT_MIN_BLOCKS_PER_SM
-#define MT_MIN_BLOCKS_PER_SM 8  // occupancy hint for the batch kernels: caps registers at 64
-#endif
-
-// Kernel flavours.  OP_PASS_* serve one class of a partitioned mixed batch and
-// compile only that class's code (smaller kernels, fewer instruction-cache
-// misses than OP_MIXED, which handles every kind).
-enum op_kind : int {
-  OP_FIND = 0, OP_INSERT = 1, OP_UPSERT = 2, OP_UPDATE = 3, OP_ERASE = 4, OP_MIXED = 5,
-  OP_PASS_INSERT = 6, OP_PASS_UPDERASE = 7
-};
-template <int OP> constexpr bool op_finds = OP == OP_FIND || OP == OP_MIXED;
-template <int OP> constexpr bool op_inserts = OP == OP_INSERT || OP == OP_UPSERT || OP == OP_MIXED || OP == OP_PASS_INSERT;
-template <int OP> constexpr bool op_updates = OP == OP_UPDATE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
-template <int OP> constexpr bool op_erases = OP == OP_ERASE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
-
-struct batch_args {
-  const uint8_t* types;
-  const uint32_t* keys;
-  const uint32_t* key_lengths;
-  uint32_t* values;              // insert/update: input, find: output
-  const uint32_t* value_lengths_in;
-  uint32_t* value_lengths_out;
-  bool* results;
-  const uint32_t* index;  // optional request subset
-  const uint32_t* n_dev;  // optional device-side request count (with index)
-  uint32_t max_key_length;
-  uint32_t max_value_length;
-  uint32_t n;
-};
 
 // Split a mixed batch into its finds and its writes (insert/update/erase):
 // one atomic per warp and class.  Order inside a class is arbitrary (requests
@@ -117,57 +81,6 @@ __global__ void partition3_kernel(const uint8_t* types, uint32_t n, uint32_t* fi
   }
 }
 
-struct scan_args {
-  const uint32_t* lower;
-  const uint32_t* lower_lengths;
-  const uint32_t* upper;
-  const uint32_t* upper_lengths;
-  uint32_t* counts;
-  uint32_t* values;
-  uint32_t* value_lengths;
-  uint32_t* out_keys;
-  uint32_t* out_key_lengths;
-  scan_frame* frames;
-  uint32_t max_key_length;
-  uint32_t max_value_length;
-  uint32_t max_count;
-  uint32_t n;
-  uint32_t use_upper;
-};
-
-// One request of any kind, executed by the whole tile.
-template <int T, int OP, bool CONC>
-MT_DEV void run_request(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const batch_args& a,
-                        uint32_t j, uint32_t kind, uint32_t klen, uint32_t vlen, uint32_t& res, uint32_t& vout) {
-  const uint32_t* key = a.keys + (size_t)j * a.max_key_length;
-  if constexpr (op_finds<OP>) {
-    if (kind == MT_REQ_FIND) {
-      uint32_t* out = a.values ? a.values + (size_t)j * a.max_value_length : nullptr;
-      vout = coop_find<T, CONC>(t, tv, key, klen, out, a.max_value_length);
-      return;
-    }
-  }
-  if constexpr (op_inserts<OP>) {
-    if (kind == MT_REQ_INSERT) {
-      const uint32_t* val = a.values + (size_t)j * a.max_value_length;
-      const int r = (OP == OP_UPSERT) ? coop_insert<T, true>(t, tv, cache, key, klen, val, vlen)
-                                      : coop_insert<T, false>(t, tv, cache, key, klen, val, vlen);
-      res = (r == R_OK) ? 1u : 0u;
-      return;
-    }
-  }
-  if constexpr (op_updates<OP>) {
-    if (kind == MT_REQ_UPDATE) {
-      const uint32_t* val = a.values + (size_t)j * a.max_value_length;
-      res = (coop_update<T>(t, tv, cache, key, klen, val, vlen) == R_OK) ? 1u : 0u;
-      return;
-    }
-  }
-  if constexpr (op_erases<OP>) {
-    if (kind == MT_REQ_ERASE) res = (coop_erase<T>(t, tv, key, klen) == R_OK) ? 1u : 0u;
-  }
-}
-
 template <int T, int OP, bool CONC>
 __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batch_kernel(tree_view tv, batch_args a) {
   tile<T> t;
@@ -175,49 +88,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batch_kernel(tre
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   slab_cache<T> cache;
   cache.init(tv.pool, tile_id);
-  // With a.index the kernel serves requests a.index[0 .. *a.n_dev) (a subset
-  // produced by partition_kernel); otherwise requests 0 .. a.n.
-  const uint32_t n = a.n_dev ? *a.n_dev : a.n;
-  for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
-    if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
-    const uint32_t pos = base + t.rank;
-    const bool valid = pos < n;
-    const uint32_t i = (valid && a.index) ? a.index[pos] : pos;
-    uint32_t kind = 0, klen = 0, vlen = 0;
-    if (valid) {
-      if constexpr (OP == OP_MIXED || OP == OP_PASS_UPDERASE) kind = a.types[i];
-      else if constexpr (OP == OP_FIND) kind = MT_REQ_FIND;
-      else if constexpr (OP == OP_INSERT || OP == OP_UPSERT || OP == OP_PASS_INSERT) kind = MT_REQ_INSERT;
-      else if constexpr (OP == OP_UPDATE) kind = MT_REQ_UPDATE;
-      else kind = MT_REQ_ERASE;
-      klen = a.key_lengths ? a.key_lengths[i] : a.max_key_length;
-      if (kind == MT_REQ_INSERT || kind == MT_REQ_UPDATE)
-        vlen = a.value_lengths_in ? a.value_lengths_in[i] : a.max_value_length;
-    }
-    // Lengths beyond the row stride (or unknown kinds) would read outside the
-    // caller's buffers: such requests are skipped and reported.
-    const bool bad = valid && (klen > a.max_key_length || vlen > a.max_value_length || kind > MT_REQ_UPDATE);
-    if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
-    uint32_t res = 0, vout = 0;
-    const uint32_t nreq = min((uint32_t)T, n - base);
-    for (uint32_t r = 0; r < nreq; ++r) {
-      if (t.shfl((uint32_t)bad, (int)r)) continue;
-      const uint32_t j = t.shfl(i, (int)r);
-      const uint32_t k = t.shfl(kind, (int)r);
-      const uint32_t kl = t.shfl(klen, (int)r);
-      const uint32_t vl = t.shfl(vlen, (int)r);
-      uint32_t rr = 0, vo = 0;
-      run_request<T, OP, CONC>(t, tv, cache, a, j, k, kl, vl, rr, vo);
-      if (t.rank == r) { res = rr; vout = vo; }
-    }
-    if (valid) {
-      if (kind == MT_REQ_FIND) {
-        if (a.value_lengths_out) a.value_lengths_out[i] = vout;
-      } else if (a.results) {
-        a.results[i] = res != 0u;
-      }
-    }
-  }
+  serve_requests<T, OP, CONC>(t, tv, cache, a, tile_id, num_tiles);
   cache.release(t, tv.pool);
 }
 
@@ -329,26 +200,24 @@ __global__ void reclaim_kernel(pool_view p) {
 
 }  // namespace mtb
 
+namespace mtb {
+bool host_valid_tile(uint32_t ts) { return ts == 4 || ts == 8 || ts == 16 || ts == 32; }
+int host_max_blocks_per_sm(const void* fn, int block, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, smem) != cudaSuccess || b <= 0) b = 1;
+  return b;
+}
+int host_launch_reclaim(mt_masstree* t, cudaStream_t s) {
+  reclaim_kernel<<<kShards, 256, 0, s>>>(t->tv.pool);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
+}
+}  // namespace mtb
+
 // ------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------
 
 using namespace mtb;
-
-struct mt_masstree {
-  int device = 0;
-  int sms = 0;
-  uint32_t tile_size = 8;        // finds and scans
-  uint32_t write_tile_size = 8;  // inserts, updates, erases
-  uint32_t blocks_per_sm = 0;    // 0 = occupancy limit
-  uint32_t* split_idx = nullptr; // mixed-batch partition scratch
-  uint32_t split_cap = 0;
-  void* mem = nullptr;
-  tree_view tv{};
-  scan_frame* frames = nullptr;
-  size_t frames_tiles = 0;
-  uint32_t* h_err = nullptr;  // pinned
-};
 
 namespace {
 
@@ -417,6 +286,7 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   if (n <= t->split_cap) return MT_OK;
   if (cudaStreamSynchronize(s) != cudaSuccess) return MT_ERR_CUDA;
   if (t->split_idx) cudaFree(t->split_idx);
+  if (t->batches_mem) cudaFree(t->batches_mem);
   t->split_idx = nullptr;
   t->split_cap = 0;
   // [counts(32 words, one line)] [find indices n] [insert indices n] [update/erase indices n]
@@ -490,7 +360,7 @@ int launch_scan(mt_masstree* t, const scan_args& a, cudaStream_t s) {
   }
 }
 
-bool valid_tile(uint32_t ts) { return ts == 4 || ts == 8 || ts == 16 || ts == 32; }
+bool valid_tile(uint32_t ts) { return host_valid_tile(ts); }
 
 int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
   if (!out || !valid_tile(tile_size)) return MT_ERR_INVALID_ARG;

@@ -46,7 +46,7 @@ constexpr ld_order kConc = MT_CONC_LOAD;
 // owning entry was read with kConc, from L2.
 constexpr ld_order kConcSuffix = ld_order::RELAXED;
 
-enum op_result : int { R_ERR = -1, R_FAIL = 0, R_OK = 1 };
+enum op_result : int { RES_ERR = -1, RES_FAIL = 0, RES_OK = 1 };
 
 struct tree_view {
   pool_view pool;
@@ -413,12 +413,12 @@ MT_DEV int replace_value(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
   uint32_t nv, ns;
   if (!make_value(t, p, cache, val, vlen, nv, ns)) {
     unlock_node(t, p, nd.idx);
-    return R_ERR;
+    return RES_ERR;
   }
   nd.set_entry(t, e, nv, ns);
   publish_unlock(t, p, nd);
   if (old_state == KS_LONGVAL) suffix_retire<T, kConcSuffix>(t, p, old_val);
-  return R_OK;
+  return RES_OK;
 }
 
 // Replace a SUFFIX entry whose key rest equals K with a chain holding K + val.
@@ -432,11 +432,11 @@ MT_DEV int replace_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& c
   vs.ptr = val;
   vs.len = vlen;
   const uint32_t nv = suffix_create<T, kConcSuffix>(t, p, cache, ks, vs);
-  if (nv == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+  if (nv == kInvalid) { unlock_node(t, p, nd.idx); return RES_ERR; }
   nd.set_entry(t, e, nv, KS_SUFFIX);
   publish_unlock(t, p, nd);
   suffix_retire<T, kConcSuffix>(t, p, old_chain);
-  return R_OK;
+  return RES_OK;
 }
 
 // Entry payload for a key tail: (slice at position m of K, state, value).
@@ -485,11 +485,11 @@ MT_DEV int split_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& cac
   newK.ptr = K; newK.len = lk;
   newV.ptr = val; newV.len = vlen;
   uint32_t so, sto, vo, sn, stn, vn;
-  if (!make_tail_entry(t, p, cache, oldK, ls, m, oldV, so, sto, vo)) { unlock_node(t, p, nd.idx); return R_ERR; }
-  if (!make_tail_entry(t, p, cache, newK, lk, m, newV, sn, stn, vn)) { unlock_node(t, p, nd.idx); return R_ERR; }
+  if (!make_tail_entry(t, p, cache, oldK, ls, m, oldV, so, sto, vo)) { unlock_node(t, p, nd.idx); return RES_ERR; }
+  if (!make_tail_entry(t, p, cache, newK, lk, m, newV, sn, stn, vn)) { unlock_node(t, p, nd.idx); return RES_ERR; }
   // Doubleton layer root.
   const uint32_t dslab = cache.allocate(t, p);
-  if (dslab == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+  if (dslab == kInvalid) { unlock_node(t, p, nd.idx); return RES_ERR; }
   node<T> ln;
   make_layer_root(t, ln, dslab);
   if (pos_less(so, ks_more(sto), sn, ks_more(stn))) {
@@ -504,7 +504,7 @@ MT_DEV int split_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& cac
   uint32_t below = dslab;
   for (int i = (int)m - 1; i >= 0; --i) {
     const uint32_t s = cache.allocate(t, p);
-    if (s == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+    if (s == kInvalid) { unlock_node(t, p, nd.idx); return RES_ERR; }
     make_layer_root(t, ln, s);
     ln.insert_at(t, 0, K[i], below, KS_LINK);
     publish_new(t, p, ln);
@@ -513,7 +513,7 @@ MT_DEV int split_suffix(const tile<T>& t, const pool_view& p, slab_cache<T>& cac
   nd.set_entry(t, e, below, KS_LINK);
   publish_unlock(t, p, nd);
   suffix_retire<T, kConcSuffix>(t, p, h.idx);
-  return R_OK;
+  return RES_OK;
 }
 
 // ---- insert ------------------------------------------------------------------------
@@ -524,7 +524,7 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
   const pool_view& p = tv.pool;
   if (klen == 0u || vlen > kMaxLen16 || klen > kMaxLen16) {
     if (t.leader()) record_error(p, ERR_INVALID_ARG);
-    return R_ERR;
+    return RES_ERR;
   }
   uint32_t root = tv.root, hops = 0;
   node<T> nd;
@@ -533,7 +533,7 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
     const bool more = layer + 1u < klen;
     uint32_t link = kInvalid;
     const int r = descend_split(t, p, cache, root, slice, more, nd, link, hops);
-    if (r < 0) return R_ERR;
+    if (r < 0) return RES_ERR;
     if (r == 1) { root = link; ++layer; continue; }
     const int e = nd.match(t, slice, more);
     if (e >= 0) {
@@ -541,17 +541,17 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
       const uint32_t v = nd.val_at(t, (uint32_t)e);
       if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
       if (st == KS_VALUE || st == KS_LONGVAL) {
-        if (!UPSERT) { unlock_node(t, p, nd.idx); return R_FAIL; }
+        if (!UPSERT) { unlock_node(t, p, nd.idx); return RES_FAIL; }
         return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
       }
       // SUFFIX entry: same key, or a different key sharing this slice.
-      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);
       const uint32_t lk = klen - layer - 1u;
       const cmp_result c = suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk);
       if (c.sign == 0) {
-        if (!UPSERT) { unlock_node(t, p, nd.idx); return R_FAIL; }
+        if (!UPSERT) { unlock_node(t, p, nd.idx); return RES_FAIL; }
         return replace_suffix(t, p, cache, nd, (uint32_t)e, v, key + layer + 1u, lk, val, vlen);
       }
       return split_suffix(t, p, cache, nd, (uint32_t)e, h, c.first_diff, key + layer + 1u, lk, val, vlen);
@@ -566,16 +566,16 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
       vs.len = vlen;
       nv = suffix_create<T, kConcSuffix>(t, p, cache, ks, vs);
       ns = KS_SUFFIX;
-      if (nv == kInvalid) { unlock_node(t, p, nd.idx); return R_ERR; }
+      if (nv == kInvalid) { unlock_node(t, p, nd.idx); return RES_ERR; }
     } else if (!make_value(t, p, cache, val, vlen, nv, ns)) {
       unlock_node(t, p, nd.idx);
-      return R_ERR;
+      return RES_ERR;
     }
     nd.insert_at(t, nd.lower_pos(t, slice, more), slice, nv, ns);
     publish_unlock(t, p, nd);
-    return R_OK;
+    return RES_OK;
   }
-  return R_ERR;
+  return RES_ERR;
 }
 
 // ---- lock-free presence check ------------------------------------------------------
@@ -610,40 +610,40 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
   const pool_view& p = tv.pool;
   if (klen == 0u || vlen > kMaxLen16) {
     if (t.leader()) record_error(p, ERR_INVALID_ARG);
-    return R_ERR;
+    return RES_ERR;
   }
   uint32_t root = tv.root, hops = 0;
   node<T> nd;
   for (uint32_t layer = 0; layer < klen;) {
     const uint32_t slice = key[layer];
     const bool more = layer + 1u < klen;
-    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return R_ERR;
+    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return RES_ERR;
     if (more) {
       const int e = nd.match(t, slice, true);
       if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
     }
     uint32_t v0 = kInvalid;
-    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return R_FAIL;
-    if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
+    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return RES_FAIL;
+    if (!lock_border(t, p, slice, nd, hops)) return RES_ERR;
     const int e = nd.match(t, slice, more);
-    if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
+    if (e < 0) { unlock_node(t, p, nd.idx); return RES_FAIL; }
     const uint32_t st = ks_get(nd.ks, (uint32_t)e);
     const uint32_t v = nd.val_at(t, (uint32_t)e);
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
     if (st == KS_VALUE || st == KS_LONGVAL) return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
-    if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+    if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
     const uint32_t lk = klen - layer - 1u;
     if (v != v0) {  // the chain changed since the lock-free check: compare again
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);
       if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
         unlock_node(t, p, nd.idx);
-        return R_FAIL;
+        return RES_FAIL;
       }
     }
     return replace_suffix(t, p, cache, nd, (uint32_t)e, v, key + layer + 1u, lk, val, vlen);
   }
-  return R_FAIL;
+  return RES_FAIL;
 }
 
 // ---- erase --------------------------------------------------------------------------
@@ -651,41 +651,41 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
 template <int T>
 MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key, uint32_t klen) {
   const pool_view& p = tv.pool;
-  if (klen == 0u) return R_FAIL;
+  if (klen == 0u) return RES_FAIL;
   uint32_t root = tv.root, hops = 0;
   node<T> nd;
   for (uint32_t layer = 0; layer < klen;) {
     const uint32_t slice = key[layer];
     const bool more = layer + 1u < klen;
-    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return R_ERR;
+    if (!descend<T, kConc>(t, p, root, slice, nd, hops)) return RES_ERR;
     if (more) {
       const int e = nd.match(t, slice, true);
       if (e >= 0 && ks_get(nd.ks, (uint32_t)e) == KS_LINK) { root = nd.val_at(t, (uint32_t)e); ++layer; continue; }
     }
     uint32_t v0 = kInvalid;
-    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return R_FAIL;
-    if (!lock_border(t, p, slice, nd, hops)) return R_ERR;
+    if (!present_in_image(t, p, nd, key, klen, layer, &v0)) return RES_FAIL;
+    if (!lock_border(t, p, slice, nd, hops)) return RES_ERR;
     const int e = nd.match(t, slice, more);
-    if (e < 0) { unlock_node(t, p, nd.idx); return R_FAIL; }
+    if (e < 0) { unlock_node(t, p, nd.idx); return RES_FAIL; }
     const uint32_t st = ks_get(nd.ks, (uint32_t)e);
     const uint32_t v = nd.val_at(t, (uint32_t)e);
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
     if (st == KS_SUFFIX && v != v0) {
-      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return R_ERR; }
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);
       const uint32_t lk = klen - layer - 1u;
       if (h.klen != lk || suffix_compare<T, kConcSuffix>(t, p, h, key + layer + 1u, lk).sign != 0) {
         unlock_node(t, p, nd.idx);
-        return R_FAIL;
+        return RES_FAIL;
       }
     }
     nd.remove_at(t, (uint32_t)e);
     publish_unlock(t, p, nd);
     if (st != KS_VALUE) suffix_retire<T, kConcSuffix>(t, p, v);
-    return R_OK;
+    return RES_OK;
   }
-  return R_FAIL;
+  return RES_FAIL;
 }
 
 // ---- scan ----------------------------------------------------------------------------

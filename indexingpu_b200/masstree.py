@@ -26,7 +26,7 @@ import ctypes
 from . import _lib
 
 REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
-FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS = 1, 2, 4, 8
+FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS, FLAG_BUCKET_KEYS = 1, 2, 4, 8, 16
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
@@ -146,6 +146,19 @@ class GpuMasstree:
                                       num_requests, FLAG_SINGLE_PASS if single_pass else 0, _stream(stream))
         self._check(rc, "mt_mixed_batch")
 
+    # -- many sub-batches in one persistent launch --------------------------------
+    def reserve_batches(self, max_subbatches, max_total_requests):
+        self._check(self._lib.mt_batches_reserve(self._h, max_subbatches, max_total_requests), "mt_batches_reserve")
+
+    def mixed_batches(self, descriptors, num_subbatches, max_key_length, max_value_length, stream=0,
+                      bucket_keys=False):
+        """Serve num_subbatches mixed batches in order in one persistent launch.
+        `descriptors` is a device tensor holding mt_subbatch records (see
+        pack_subbatches)."""
+        rc = self._lib.mt_mixed_batches(self._h, _ptr(descriptors), num_subbatches, max_key_length,
+                                        max_value_length, FLAG_BUCKET_KEYS if bucket_keys else 0, _stream(stream))
+        self._check(rc, "mt_mixed_batches")
+
     # -- status ---------------------------------------------------------------------
     def sync(self, stream=0):
         """Wait for the stream; raise MasstreeError if a device error was recorded."""
@@ -177,3 +190,18 @@ def line_atomicity_selftest(tile_size, nlines=64, iters=20000):
     if rc != 0:
         raise MasstreeError(rc, "mt_selftest_line_atomicity")
     return int(r.value), int(t.value)
+
+
+def pack_subbatches(subbatches):
+    """Pack sub-batches (dicts of device tensors: types, keys, lens, vals, vlens,
+    results; lens and results may be None) into the mt_subbatch layout; returns
+    a uint8 numpy array of 56 bytes per sub-batch, to be copied to the device."""
+    import numpy as np
+    rec = np.dtype([("types", "<u8"), ("keys", "<u8"), ("lens", "<u8"), ("vals", "<u8"), ("vlens", "<u8"),
+                    ("results", "<u8"), ("n", "<u4"), ("reserved", "<u4")])
+    arr = np.zeros(len(subbatches), dtype=rec)
+    for i, sb in enumerate(subbatches):
+        for f in ("types", "keys", "lens", "vals", "vlens", "results"):
+            arr[i][f] = _ptr(sb.get(f)) or 0
+        arr[i]["n"] = int(sb["n"])
+    return arr.view(np.uint8)
