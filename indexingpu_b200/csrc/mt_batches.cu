@@ -10,7 +10,8 @@
 //      optionally split into short and long keys (filled from the two ends of
 //      the class's index region, so each class is served short keys first);
 //   3. batches_persistent_kernel: a cooperative grid walks the sub-batches in
-//      order and serves each class with a grid barrier between classes.
+//      order with one grid barrier between sub-batches; inside a sub-batch the
+//      tiles flow from finds to inserts to updates and erases without one.
 // Sub-batch k+1 observes every effect of sub-batch k, as with one host call per
 // sub-batch; inside a sub-batch the classes run finds, inserts, then updates
 // and erases (one of the orders a mixed batch allows).  Nothing in the call
@@ -104,9 +105,8 @@ __global__ void batches_partition_kernel(batches_view b) {
   }
 }
 
-template <int T, int OP>
-MT_DEV void serve_class(const tile<T>& t, const tree_view& tv, slab_cache<T>& cache, const batches_view& b,
-                        uint32_t sb, uint32_t cls) {
+// Arguments of class cls of sub-batch sb (index region filled from both ends).
+MT_DEV batch_args class_args(const batches_view& b, uint32_t sb, uint32_t cls) {
   const mt_subbatch d = b.sub[sb];
   batch_args a{};
   a.types = d.request_types;
@@ -122,30 +122,23 @@ MT_DEV void serve_class(const tile<T>& t, const tree_view& tv, slab_cache<T>& ca
   a.region = d.num_requests;
   a.max_key_length = b.max_key_length;
   a.max_value_length = b.max_value_length;
-  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
-  const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
-  serve_requests<T, OP, true>(t, tv, cache, a, tile_id, num_tiles);
+  return a;
 }
 
+// One grid barrier per sub-batch: sub-batch sb+1 starts after every request of
+// sub-batch sb has finished; inside a sub-batch the classes flow without one.
 template <int TF, int TW>
 __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_persistent_kernel(tree_view tv,
                                                                                           batches_view b) {
   if (b.status[0]) return;  // uniform over the grid: no barrier is skipped by a subset
   cg::grid_group grid = cg::this_grid();
-  tile<TF> tf;
-  tile<TW> tw;
-  slab_cache<TF> fcache;  // unused by finds; required by the serving interface
   slab_cache<TW> wcache;
-  fcache.init(tv.pool, 0u);
   wcache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / TW);
   for (uint32_t sb = 0; sb < b.nsub; ++sb) {
-    serve_class<TF, OP_FIND>(tf, tv, fcache, b, sb, 0u);
-    grid.sync();
-    serve_class<TW, OP_PASS_INSERT>(tw, tv, wcache, b, sb, 1u);
-    grid.sync();
-    serve_class<TW, OP_PASS_UPDERASE>(tw, tv, wcache, b, sb, 2u);
+    serve_mixed_classes<TF, TW>(tv, wcache, class_args(b, sb, 0u), class_args(b, sb, 1u), class_args(b, sb, 2u));
     grid.sync();
   }
+  tile<TW> tw;
   wcache.release(tw, tv.pool);
 }
 
@@ -176,7 +169,7 @@ int launch_persistent(mt_masstree* t, const batches_view& b, cudaStream_t s) {
 
 template <int TF>
 int launch_persistent_tf(mt_masstree* t, const batches_view& b, cudaStream_t s) {
-  switch (t->write_tile_size) {
+  switch (t->write_tile_size <= 16 ? 16u : 32u) {
     case 16: return launch_persistent<TF, 16>(t, b, s);
     case 32: return launch_persistent<TF, 32>(t, b, s);
     default: return MT_ERR_INVALID_ARG;

@@ -295,12 +295,45 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   return MT_OK;
 }
 
-// A mixed batch as four launches: partition by kind, then every find with the
-// find tile width, then the inserts, then the updates and erases, both with the
+// Partitioned mixed batch: the classes of one batch in one launch.
+template <int TF, int TW>
+__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) mixed_classes_kernel(tree_view tv, batch_args f,
+                                                                                     batch_args i, batch_args u) {
+  slab_cache<TW> wcache;
+  wcache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / TW);
+  serve_mixed_classes<TF, TW>(tv, wcache, f, i, u);
+  tile<TW> tw;
+  wcache.release(tw, tv.pool);
+}
+
+template <int TF, int TW>
+int launch_mixed_classes(mt_masstree* t, const batch_args& f, const batch_args& i, const batch_args& u,
+                         cudaStream_t s) {
+  const void* fn = (const void*)mixed_classes_kernel<TF, TW>;
+  const int grid = grid_for(t, fn);
+  mixed_classes_kernel<TF, TW><<<grid, kBlock, 0, s>>>(t->tv, f, i, u);
+  return cuda_status(cudaGetLastError());
+}
+
+// Mixed batches serve writes with 16- or 32-lane tiles (narrower write tiles,
+// allowed for plain insert/update/erase calls, are widened to 16 here).
+template <int TF>
+int launch_mixed_classes_tf(mt_masstree* t, const batch_args& f, const batch_args& i, const batch_args& u,
+                            cudaStream_t s) {
+  switch (t->write_tile_size <= 16 ? 16u : 32u) {
+    case 16: return launch_mixed_classes<TF, 16>(t, f, i, u, s);
+    case 32: return launch_mixed_classes<TF, 32>(t, f, i, u, s);
+    default: return MT_ERR_INVALID_ARG;
+  }
+}
+
+// A mixed batch as three launches: reclaim, partition by class (finds,
+// inserts, updates+erases), then one launch in which every tile serves finds
+// with the find tile width, then inserts, then updates and erases with the
 // write tile width.  Requests of one mixed batch have no defined order, so
-// serving them class by class is one of the orders the reference allows; it
-// removes the divergence between the tiles of a warp and keeps each kernel's
-// code small.
+// class by class is one of the orders the reference allows; it removes the
+// divergence between the tiles of a warp and keeps the code each warp runs at
+// a time small.
 int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   if (a.n == 0) return MT_OK;
   int rc = ensure_split_scratch(t, a.n, s);
@@ -315,19 +348,20 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   partition3_kernel<<<std::max(1, std::min(t->sms * 8, (int)((a.n + 255) / 256))), 256, 0, s>>>(
       a.types, a.n, find_idx, insert_idx, upderase_idx, counts);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
-  batch_args f = a;
+  batch_args f = a, i = a, u = a;
   f.index = find_idx;
   f.n_dev = counts;
-  rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, s);
-  if (rc) return rc;
-  batch_args w = a;
-  w.index = insert_idx;
-  w.n_dev = counts + 1;
-  rc = launch_batch_tile<OP_PASS_INSERT, true>(t, t->write_tile_size, w, s);
-  if (rc) return rc;
-  w.index = upderase_idx;
-  w.n_dev = counts + 2;
-  return launch_batch_tile<OP_PASS_UPDERASE, true>(t, t->write_tile_size, w, s);
+  i.index = insert_idx;
+  i.n_dev = counts + 1;
+  u.index = upderase_idx;
+  u.n_dev = counts + 2;
+  switch (t->tile_size) {
+    case 4: return launch_mixed_classes_tf<4>(t, f, i, u, s);
+    case 8: return launch_mixed_classes_tf<8>(t, f, i, u, s);
+    case 16: return launch_mixed_classes_tf<16>(t, f, i, u, s);
+    case 32: return launch_mixed_classes_tf<32>(t, f, i, u, s);
+    default: return MT_ERR_INVALID_ARG;
+  }
 }
 
 template <int T, bool CONC>

@@ -177,3 +177,27 @@ int host_max_blocks_per_sm(const void* fn, int block, size_t smem);
 int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
 bool host_valid_tile(uint32_t ts);
 }  // namespace mtb
+
+namespace mtb {
+
+// The three request classes of one mixed batch, served by every tile of the
+// launch in turn with no barrier between them: finds with TF-lane tiles, then
+// inserts, then updates and erases with TW-lane tiles.  Requests of one mixed
+// batch have no defined order, so a tile may start on inserts while others
+// still serve finds; only the tail of the whole batch is waited for.
+template <int TF, int TW>
+MT_DEV void serve_mixed_classes(const tree_view& tv, slab_cache<TW>& wcache, const batch_args& finds,
+                                const batch_args& inserts, const batch_args& upderases) {
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  {
+    tile<TF> t;
+    slab_cache<TF> unused;  // finds never allocate
+    serve_requests<TF, OP_FIND, true>(t, tv, unused, finds, gtid / TF, nthreads / TF);
+  }
+  tile<TW> t;
+  serve_requests<TW, OP_PASS_INSERT, true>(t, tv, wcache, inserts, gtid / TW, nthreads / TW);
+  serve_requests<TW, OP_PASS_UPDERASE, true>(t, tv, wcache, upderases, gtid / TW, nthreads / TW);
+}
+
+}  // namespace mtb
