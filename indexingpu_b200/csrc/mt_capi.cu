@@ -98,17 +98,21 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(tree_view tv, scan_args a)
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   scan_frame* frames = a.frames + (size_t)tile_id * kScanDepth;
-  for (uint32_t base = tile_id * T; base < a.n; base += num_tiles * T) {
+  // Queries per tile and round: T on large batches, fewer on small ones so that
+  // every tile gets work (as in serve_requests).
+  const uint32_t per = max(1u, min((uint32_t)T, (a.n + num_tiles - 1u) / num_tiles));
+  for (uint32_t base = tile_id * per; base < a.n; base += num_tiles * per) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
     const uint32_t i = base + t.rank;
+    const bool valid = t.rank < per && i < a.n;
     uint32_t llen = 0, ulen = 0, cnt = 0;
-    if (i < a.n) {
+    if (valid) {
       llen = a.lower_lengths ? a.lower_lengths[i] : a.max_key_length;
       ulen = a.upper_lengths ? a.upper_lengths[i] : a.max_key_length;
     }
-    const bool bad = i < a.n && (llen > a.max_key_length || (a.use_upper && ulen > a.max_key_length));
+    const bool bad = valid && (llen > a.max_key_length || (a.use_upper && ulen > a.max_key_length));
     if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
-    const uint32_t nreq = min((uint32_t)T, a.n - base);
+    const uint32_t nreq = min(per, a.n - base);
     for (uint32_t r = 0; r < nreq; ++r) {
       if (t.shfl((uint32_t)bad, (int)r)) continue;
       const uint32_t q = base + r;
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(tree_view tv, scan_args a)
                                            a.max_count, o, frames, kScanDepth);
       if (t.rank == r) cnt = c;
     }
-    if (i < a.n && a.counts) a.counts[i] = cnt;
+    if (valid && a.counts) a.counts[i] = cnt;
   }
 }
 

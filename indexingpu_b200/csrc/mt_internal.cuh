@@ -107,10 +107,15 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
   const uint32_t nf = a.n_dev ? *a.n_dev : a.n;
   const uint32_t nb = a.n_back_dev ? *a.n_back_dev : 0u;
   const uint32_t n = nf + nb;
-  for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
+  // A tile takes `per` consecutive requests per round (one per lane, served in
+  // turn).  per = T keeps the metadata loads coalesced on large batches; on
+  // small ones per shrinks so that every tile gets work and the batch ends
+  // after one request latency instead of T of them.
+  const uint32_t per = max(1u, min((uint32_t)T, (n + num_tiles - 1u) / num_tiles));
+  for (uint32_t base = tile_id * per; base < n; base += num_tiles * per) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
     const uint32_t pos = base + t.rank;
-    const bool valid = pos < n;
+    const bool valid = t.rank < per && pos < n;
     const uint32_t i = (valid && a.index) ? a.index[pos < nf ? pos : a.region - nb + (pos - nf)] : pos;
     uint32_t kind = 0, klen = 0, vlen = 0;
     if (valid) {
@@ -128,7 +133,7 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
     const bool bad = valid && (klen > a.max_key_length || vlen > a.max_value_length || kind > MT_REQ_UPDATE);
     if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
     uint32_t res = 0, vout = 0;
-    const uint32_t nreq = min((uint32_t)T, n - base);
+    const uint32_t nreq = min(per, n - base);
     for (uint32_t r = 0; r < nreq; ++r) {
       if (t.shfl((uint32_t)bad, (int)r)) continue;
       const uint32_t j = t.shfl(i, (int)r);
