@@ -134,8 +134,24 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_persiste
   cg::grid_group grid = cg::this_grid();
   slab_cache<TW> wcache;
   wcache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / TW);
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
   for (uint32_t sb = 0; sb < b.nsub; ++sb) {
-    serve_mixed_classes<TF, TW>(tv, wcache, class_args(b, sb, 0u), class_args(b, sb, 1u), class_args(b, sb, 2u));
+    if (b.sub[sb].num_requests >= kClassBarrierMin) {
+      // Large sub-batch: one class at a time.
+      {
+        tile<TF> tf;
+        slab_cache<TF> unused;
+        serve_requests<TF, OP_FIND, true>(tf, tv, unused, class_args(b, sb, 0u), gtid / TF, nthreads / TF);
+      }
+      grid.sync();
+      tile<TW> tw;
+      serve_requests<TW, OP_PASS_INSERT, true>(tw, tv, wcache, class_args(b, sb, 1u), gtid / TW, nthreads / TW);
+      grid.sync();
+      serve_requests<TW, OP_PASS_UPDERASE, true>(tw, tv, wcache, class_args(b, sb, 2u), gtid / TW, nthreads / TW);
+    } else {
+      serve_mixed_classes<TF, TW>(tv, wcache, class_args(b, sb, 0u), class_args(b, sb, 1u), class_args(b, sb, 2u));
+    }
     grid.sync();
   }
   tile<TW> tw;

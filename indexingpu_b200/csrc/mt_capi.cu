@@ -331,10 +331,10 @@ int launch_mixed_classes_tf(mt_masstree* t, const batch_args& f, const batch_arg
   }
 }
 
-// A mixed batch as three launches: reclaim, partition by class (finds,
-// inserts, updates+erases), then one launch in which every tile serves finds
-// with the find tile width, then inserts, then updates and erases with the
-// write tile width.  Requests of one mixed batch have no defined order, so
+// A mixed batch: reclaim, partition by class (finds, inserts, updates+erases),
+// then either one launch in which every tile serves finds with the find tile
+// width, then inserts, then updates and erases with the write tile width
+// (small batches), or one launch per class (large batches).  Requests of one mixed batch have no defined order, so
 // class by class is one of the orders the reference allows; it removes the
 // divergence between the tiles of a warp and keeps the code each warp runs at
 // a time small.
@@ -359,6 +359,15 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   i.n_dev = counts + 1;
   u.index = upderase_idx;
   u.n_dev = counts + 2;
+  if (a.n >= kClassBarrierMin) {
+    // Large batch: one launch per class.
+    rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, s);
+    if (rc) return rc;
+    const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
+    rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
+    if (rc) return rc;
+    return launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, s);
+  }
   switch (t->tile_size) {
     case 4: return launch_mixed_classes_tf<4>(t, f, i, u, s);
     case 8: return launch_mixed_classes_tf<8>(t, f, i, u, s);
