@@ -151,6 +151,50 @@ int mt_batches_reserve(mt_masstree* tree, uint32_t max_subbatches, uint64_t max_
 int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t num_subbatches,
                      uint32_t max_key_length, uint32_t max_value_length, uint32_t flags, void* stream);
 
+/* Serving (mt_serve). */
+#define MT_SERVE_SERVED 0u /* device-resident request loop with continuous admission */
+#define MT_SERVE_PLAIN 1u  /* one synchronous mt_mixed_batch call per request, in arrival order */
+
+typedef struct mt_serve_plan {
+  /* Ops of every request, concatenated (device pointers; request r owns ops
+   * [request_first_op[r], request_first_op[r] + request_num_ops[r])). */
+  const uint8_t* types;
+  const uint32_t* keys;
+  const uint32_t* key_lengths; /* may be NULL */
+  uint32_t* values;
+  uint32_t* value_lengths;
+  bool* results;               /* may be NULL */
+  uint32_t max_key_length;
+  uint32_t max_value_length;
+  /* Host arrays, one entry per request, in arrival order. */
+  const uint32_t* request_first_op;
+  const uint32_t* request_num_ops;
+  const uint64_t* arrival_ns;  /* arrival time after the start of the run */
+  uint32_t num_requests;
+  uint32_t mode;               /* MT_SERVE_SERVED or MT_SERVE_PLAIN */
+  uint32_t chunk_ops;          /* ops per device work item (0 = 32) */
+  uint32_t epoch_us;           /* device time per launch of the serving loop (0 = 20000) */
+  float memory_budget;         /* admit while slabs in use stay under this share of the pool (0 = 0.9) */
+  uint32_t reserved;
+} mt_serve_plan;
+
+typedef struct mt_serve_stats {
+  uint64_t wall_ns;          /* host time from start to the last completion */
+  uint64_t requests_done;
+  uint64_t ops_done;
+  uint64_t admission_waits;  /* times an arrived request waited for slab memory */
+} mt_serve_stats;
+
+/* Serve an open-loop stream of requests: each request is admitted when its
+ * arrival time has come (and memory allows), served by the device-resident
+ * loop together with whatever else is in flight, and completed by a flag the
+ * device writes to host memory.  latency_ns[r] (host array) receives
+ * completion - arrival for request r.  Synchronous; runs on its own stream.
+ * Requests in flight together have no defined order among each other, as the
+ * requests of one reference mixed_batch.  No counterpart in the reference
+ * (its host API serves one batch per call). */
+int mt_serve(mt_masstree* tree, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats);
+
 /* mt_mixed_batch for callers that must not allocate device memory during the
  * call: code that runs while a CUDA graph is being captured (cudaMalloc is not
  * a stream operation and breaks the capture), request loops that must never

@@ -33,6 +33,7 @@ SIGNATURES = {
     "mt_status_string": (ctypes.c_char_p, [_int]),
     "mt_validate": (_int, [_p, ctypes.POINTER(_u64), ctypes.c_char_p, ctypes.c_size_t]),
     "mt_selftest_line_atomicity": (_int, [_u32, _u32, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
+    "mt_serve": (_int, [_p, _p, _p, _p]),
 }
 
 
@@ -46,6 +47,37 @@ class MtStats(ctypes.Structure):
         ("tile_size", _u32),
         ("device_error", _u32),
         ("device_error_count", _u32),
+    ]
+
+
+class MtServePlan(ctypes.Structure):
+    _fields_ = [
+        ("types", _p),
+        ("keys", _p),
+        ("key_lengths", _p),
+        ("values", _p),
+        ("value_lengths", _p),
+        ("results", _p),
+        ("max_key_length", _u32),
+        ("max_value_length", _u32),
+        ("request_first_op", _p),
+        ("request_num_ops", _p),
+        ("arrival_ns", _p),
+        ("num_requests", _u32),
+        ("mode", _u32),
+        ("chunk_ops", _u32),
+        ("epoch_us", _u32),
+        ("memory_budget", ctypes.c_float),
+        ("reserved", _u32),
+    ]
+
+
+class MtServeStats(ctypes.Structure):
+    _fields_ = [
+        ("wall_ns", _u64),
+        ("requests_done", _u64),
+        ("ops_done", _u64),
+        ("admission_waits", _u64),
     ]
 
 

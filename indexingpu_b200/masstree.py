@@ -159,6 +159,38 @@ class GpuMasstree:
                                         max_value_length, FLAG_BUCKET_KEYS if bucket_keys else 0, _stream(stream))
         self._check(rc, "mt_mixed_batches")
 
+    # -- serving ---------------------------------------------------------------------
+    def serve(self, types, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, results,
+              request_first_op, request_num_ops, arrival_ns, plain=False, chunk_ops=0, epoch_us=0,
+              memory_budget=0.0):
+        """Serve an open-loop request stream (mt_serve).  Op buffers are device
+        tensors holding every request's ops; request_first_op, request_num_ops
+        and arrival_ns (nanoseconds after the start, non-decreasing) are host
+        arrays, one entry per request.  Returns (latency_ns numpy array, stats
+        dict).  plain=True serves one synchronous mixed_batch per request."""
+        import numpy as np
+        first = np.ascontiguousarray(request_first_op, dtype=np.uint32)
+        nops = np.ascontiguousarray(request_num_ops, dtype=np.uint32)
+        arr = np.ascontiguousarray(arrival_ns, dtype=np.uint64)
+        n = len(first)
+        if len(nops) != n or len(arr) != n:
+            raise ValueError("request arrays differ in length")
+        lat = np.zeros(n, dtype=np.uint64)
+        plan = _lib.MtServePlan()
+        plan.types, plan.keys, plan.key_lengths = _ptr(types), _ptr(keys), _ptr(key_lengths)
+        plan.values, plan.value_lengths, plan.results = _ptr(values), _ptr(value_lengths), _ptr(results)
+        plan.max_key_length, plan.max_value_length = max_key_length, max_value_length
+        plan.request_first_op = first.ctypes.data
+        plan.request_num_ops = nops.ctypes.data
+        plan.arrival_ns = arr.ctypes.data
+        plan.num_requests = n
+        plan.mode = 1 if plain else 0
+        plan.chunk_ops, plan.epoch_us, plan.memory_budget = chunk_ops, epoch_us, memory_budget
+        st = _lib.MtServeStats()
+        rc = self._lib.mt_serve(self._h, ctypes.byref(plan), lat.ctypes.data, ctypes.byref(st))
+        self._check(rc, "mt_serve")
+        return lat, {f: getattr(st, f) for f, _ in _lib.MtServeStats._fields_}
+
     # -- status ---------------------------------------------------------------------
     def sync(self, stream=0):
         """Wait for the stream; raise MasstreeError if a device error was recorded."""

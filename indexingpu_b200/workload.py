@@ -236,3 +236,58 @@ def c3(n_keys, n_queries, seed=0xC3):
     lower = np.stack([(q >> U64(32)).astype(np.uint32), (q & U64(0xFFFFFFFF)).astype(np.uint32)], axis=1)
     return dict(keys=keys, lens=np.full(n_keys, 2, np.uint32), vals=vals, vlens=np.ones(n_keys, np.uint32),
                 lower=lower, lower_lens=np.full(n_queries, 2, np.uint32))
+
+
+# ---- C5 (serving) ---------------------------------------------------------------
+
+def serve_stream(c2, n_requests, rate_per_s=None, min_ops=1, max_ops=64, seed=0xC5, disjoint=False,
+                 mix=(0.5, 0.3, 0.1, 0.1), first_fresh=None):
+    """Open-loop request stream over a C2 tree of c2.n_preload keys.
+
+    Request r holds 1 + floor(log-uniform) ops in [min_ops, max_ops] of the C2
+    mix; arrivals are a Poisson process of rate_per_s requests per second
+    (None: all at time 0).  disjoint=True draws find/update/erase keys without
+    replacement from the preloaded ids (and half the finds from absent ids), so
+    no two ops of the whole stream touch the same key and every op's result is
+    independent of how requests interleave; otherwise they are Zipf(theta) as
+    in c2 batches.  Inserts always use fresh ids (from first_fresh, default
+    just above any c2.batch id range).  Returns op arrays (types, ids, keys,
+    lens, vals, vlens) and per-request first, nops, arrival_ns."""
+    r = np.arange(n_requests, dtype=np.int64)
+    u = uniform01(seed, 1, r)
+    lo, hi = np.log(min_ops), np.log(max_ops + 1)
+    nops = np.minimum(np.exp(lo + u * (hi - lo)).astype(np.int64), max_ops).astype(np.uint32)
+    first = np.concatenate([[0], np.cumsum(nops[:-1], dtype=np.int64)]).astype(np.uint32)
+    total = int(nops.sum(dtype=np.int64))
+    idx = np.arange(total, dtype=np.int64)
+    cum = np.cumsum(np.asarray(mix, np.float64))
+    v = uniform01(seed, 2, idx)
+    types = np.where(v < cum[0], REQ_FIND, np.where(v < cum[1], REQ_INSERT,
+                                                    np.where(v < cum[2], REQ_UPDATE, REQ_ERASE))).astype(np.uint8)
+    if first_fresh is None:
+        first_fresh = c2.n_preload + c2.id_space // 2
+    if first_fresh + total > c2.id_space:
+        raise ValueError("fresh ids beyond the key id space")
+    fresh = first_fresh + idx
+    if disjoint:
+        if total > c2.n_preload:
+            raise ValueError("disjoint stream needs at least as many preloaded keys as ops")
+        old = feistel_permute(idx.astype(U64), c2.n_preload, seed).astype(np.int64)
+        miss = (types == REQ_FIND) & (rnd32(seed, 3, idx) & np.uint32(1)).astype(bool)
+        ids = np.where((types == REQ_INSERT) | miss, fresh, old)
+    else:
+        ids = np.where(types == REQ_INSERT, fresh, zipf_sample(c2.n_preload, c2.theta, uniform01(seed, 4, idx)))
+    keys, lens, vals, vlens = c2.keys(ids)
+    upd = types == REQ_UPDATE
+    with np.errstate(over="ignore"):
+        newv = (vals.astype(U64) ^ U64(0x5BD1E995)).astype(np.uint32)
+    vals = np.where(upd[:, None] & (np.arange(c2.maxV)[None, :] < vlens[:, None]), newv, vals)
+    vals = np.where((types == REQ_FIND)[:, None], 0, vals).astype(np.uint32)
+    vlens = np.where(types == REQ_FIND, 0, vlens).astype(np.uint32)
+    if rate_per_s is None:
+        arrival = np.zeros(n_requests, np.uint64)
+    else:
+        gaps = -np.log1p(-uniform01(seed, 5, r)) / float(rate_per_s)
+        arrival = (np.cumsum(gaps) * 1e9).astype(np.uint64)
+    return dict(types=types, ids=ids, keys=keys, lens=lens.astype(np.uint32), vals=vals, vlens=vlens,
+                first=first, nops=nops, arrival_ns=arrival)
