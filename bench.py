@@ -51,6 +51,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
+    ap.add_argument("--sections", default="batched,served",
+                    help="extra measurements at N=1: batched (256 sub-batches, tuned persistent launch from a "
+                         "CUDA graph, against one call per sub-batch), served (request loop over 64M keys, "
+                         "latency against offered load, against one call per request); 'none' to skip")
+    ap.add_argument("--subbatches", type=int, default=256)
+    ap.add_argument("--tune-subbatches", type=int, default=16, help="sub-batches per autotuner trial")
+    ap.add_argument("--serve-keys", type=int, default=1 << 26, help="tree size for the served section")
+    ap.add_argument("--serve-requests", type=int, default=8000, help="requests per offered-load point")
+    ap.add_argument("--serve-chunk", type=int, default=0,
+                    help="ops per work item of the request loop (0: chosen per request from the backlog)")
     return ap.parse_args()
 
 
@@ -294,6 +304,14 @@ def run_ours(args, rank, world, dist):
     tree.sync(stream)
     e2e_ms = e0.elapsed_time(e1)
     stats = tree.stats()
+    extra = {}
+    wanted = set() if args.sections == "none" else set(args.sections.split(","))
+    if world == 1:
+        del host, out, dbuf
+        if "batched" in wanted:
+            extra["batched"] = run_batched(args, tree, c2, stream)
+        if "served" in wanted:
+            extra["served"] = run_served(args, tree, c2, stream)
     tree.close()
 
     # Reduce over ranks: max time.
@@ -347,7 +365,154 @@ def run_ours(args, rank, world, dist):
             "gpu_launches": 4 * args.steps,
             "pool": {"used_slabs": stats["used_slabs"], "total_slabs": stats["total_slabs"]},
         }
+        res.update(extra)
     return res
+
+
+# ---- batched and served forms ------------------------------------------------------
+
+def _dev_ops(torch, st):
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    return dict(types=d(st["types"]), keys=d(st["keys"]), lens=d(st["lens"]), vals=d(st["vals"]),
+                vlens=d(st["vlens"]), res=torch.zeros(len(st["types"]), dtype=torch.bool, device="cuda"))
+
+
+def _subbatches(dev, st):
+    subs = []
+    for f, n in zip(st["first"].tolist(), st["nops"].tolist()):
+        subs.append(dict(types=dev["types"][f:f + n], keys=dev["keys"][f:f + n], lens=dev["lens"][f:f + n],
+                         vals=dev["vals"][f:f + n], vlens=dev["vlens"][f:f + n], results=dev["res"][f:f + n],
+                         n=n))
+    return subs
+
+
+def run_batched(args, tree, c2, stream):
+    """256 mixed sub-batches of log-uniform sizes in [1K, 1M] (sizes from seed
+    0xC4, C2 op mix and key choice): one mixed_batch call per sub-batch against
+    the autotuned persistent launch (mt_mixed_batches) replayed from a CUDA
+    graph, each on its own draw of the ops (same sizes)."""
+    import torch
+    from indexingpu_b200 import autotune
+    from indexingpu_b200.masstree import pack_subbatches
+
+    base = args.preload + (1 << 30)  # fresh-key ids of this section, above every c2.batch id
+    shape = dict(min_ops=1024, max_ops=1 << 20, seed=0xC4)
+    # One call per sub-batch.
+    st = wl.serve_stream(c2, args.subbatches, op_seed=0xC4, first_fresh=base, **shape)
+    dev = _dev_ops(torch, st)
+    total = int(st["nops"].sum())
+    # Size the per-call scratch for the largest sub-batch outside the timed
+    # region (an untimed call of finds that miss: the tree does not change).
+    n_max = int(st["nops"].max())
+    tree.mixed_batch(torch.full((n_max,), wl.REQ_FIND, dtype=torch.uint8, device="cuda"),
+                     torch.zeros((n_max, MAXK), dtype=torch.uint32, device="cuda"), MAXK,
+                     torch.full((n_max,), MAXK, dtype=torch.uint32, device="cuda"),
+                     torch.zeros((n_max, MAXV), dtype=torch.uint32, device="cuda"), MAXV,
+                     torch.zeros(n_max, dtype=torch.uint32, device="cuda"), None, n_max, stream=stream)
+    tree.sync(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for sb in _subbatches(dev, st):
+        tree.mixed_batch(sb["types"], sb["keys"], MAXK, sb["lens"], sb["vals"], MAXV, sb["vlens"], sb["results"],
+                         sb["n"], stream=stream)
+    e1.record(stream)
+    tree.sync(stream)
+    per_call = total / (e0.elapsed_time(e1) / 1e3) / 1e6
+    del dev
+
+    # Autotune on smaller cases of the same size distribution, fresh ops each.
+    def make_case(i):
+        cst = wl.serve_stream(c2, args.tune_subbatches, min_ops=1024, max_ops=1 << 20, seed=0xC4 + 7,
+                              op_seed=0xC4 + 100 + i, first_fresh=base + (1 << 27) + i * (1 << 23))
+        cdev = _dev_ops(torch, cst)
+        desc = torch.from_numpy(pack_subbatches(_subbatches(cdev, cst))).cuda()
+        return dict(descriptors=desc, num_subbatches=len(cst["nops"]), total=int(cst["nops"].sum()),
+                    max_key_length=MAXK, max_value_length=MAXV, keep=cdev)
+
+    best, trials = autotune.tune(tree, make_case, stream=stream)
+
+    # The tuned form: one persistent launch for all sub-batches, from a graph.
+    st = wl.serve_stream(c2, args.subbatches, op_seed=0xC4 + 1, first_fresh=base + (1 << 26), **shape)
+    dev = _dev_ops(torch, st)
+    desc = torch.from_numpy(pack_subbatches(_subbatches(dev, st))).cuda()
+    total_b = int(st["nops"].sum())
+    autotune.apply(tree, best)
+    tree.reserve_batches(args.subbatches, total_b)
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        tree.mixed_batches(desc, args.subbatches, MAXK, MAXV, stream=side, bucket_keys=best["bucketing"])
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        e0.record(side)
+        g.replay()
+        e1.record(side)
+    tree.sync(side)
+    batched = total_b / (e0.elapsed_time(e1) / 1e3) / 1e6
+    del g, dev
+    autotune.apply(tree, dict(find_tile=args.tile, write_tile=args.write_tile, blocks_per_sm=args.blocks_per_sm))
+    return {"workload": f"{args.subbatches} mixed sub-batches, sizes log-uniform in [1K, 1M] (seed 0xC4), "
+                        "C2 mix and Zipf(0.99) key choice over the preloaded keys",
+            "requests": [total, total_b],
+            "per_call_mops": round(per_call, 2), "batched_graph_mops": round(batched, 2),
+            "batched_over_per_call": round(batched / per_call, 3),
+            "tuned": best, "trials": trials,
+            "note": "each form runs its own draw of the ops (same sizes) on the live tree"}
+
+
+def run_served(args, tree, c2, stream):
+    """Open-loop request streams over the tree grown to --serve-keys keys:
+    requests of 1-4096 ops (log-uniform, C2 mix), Poisson arrivals at 10..100%
+    of the loop's measured peak, latency from arrival to the host seeing the
+    completion; beside it one synchronous mixed_batch call per request."""
+    import torch
+    t_grow = time.time()
+    step = 1 << 20
+    for s0 in range(args.preload, args.serve_keys, step):
+        ids = np.arange(s0, min(args.serve_keys, s0 + step))
+        k, l, v, vl = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in gen_keys(c2, ids))
+        tree.insert(k, MAXK, l, v, MAXV, vl, len(ids), stream=stream)
+    tree.sync(stream)
+    t_grow = time.time() - t_grow
+    c5 = wl.C2(n_preload=args.serve_keys, seed=c2.seed)
+    fresh0 = args.serve_keys + (1 << 31)
+    n = args.serve_requests
+
+    def once(i, rate, plain=False, n_req=n):
+        st = wl.serve_stream(c5, n_req, rate_per_s=rate, min_ops=1, max_ops=4096, seed=0xC5 + i,
+                             first_fresh=fresh0 + i * (1 << 24))
+        dev = _dev_ops(torch, st)
+        lat, stats = tree.serve(dev["types"], dev["keys"], MAXK, dev["lens"], dev["vals"], MAXV, dev["vlens"],
+                                dev["res"], st["first"], st["nops"], st["arrival_ns"], plain=plain,
+                                chunk_ops=args.serve_chunk)
+        tree.sync(stream)
+        ops = int(st["nops"].sum())
+        p = np.percentile(lat / 1e3, [50, 99, 99.9])
+        return {"offered_req_s": None if rate is None else round(rate, 1), "requests": n_req, "ops": ops,
+                "req_s": round(n_req / (stats["wall_ns"] / 1e9), 1), "mops": round(ops / stats["wall_ns"] * 1e3, 3),
+                "p50_us": round(float(p[0]), 1), "p99_us": round(float(p[1]), 1), "p999_us": round(float(p[2]), 1),
+                "admission_waits": stats["admission_waits"]}
+
+    peak = once(0, None)
+    curve = []
+    for j, frac in enumerate((0.1, 0.25, 0.5, 0.75, 0.9, 1.0)):
+        r = once(1 + j, frac * peak["req_s"])
+        r["load"] = frac
+        curve.append(r)
+    n_plain = max(200, n // 4)
+    plain_peak = once(10, None, plain=True, n_req=n_plain)
+    rate_eq = 0.5 * plain_peak["req_s"]
+    plain_half = once(11, rate_eq, plain=True, n_req=n_plain)
+    served_half = once(12, rate_eq, n_req=n_plain)
+    return {"workload": f"requests of 1-4096 ops (log-uniform, C2 mix, Zipf(0.99) over {args.serve_keys} keys), "
+                        "Poisson arrivals (seed 0xC5+i); latency = arrival to completion seen by the host",
+            "tree_keys": args.serve_keys, "grow_s": round(t_grow, 1), "chunk_ops": args.serve_chunk,
+            "served_peak": peak, "served_curve": curve,
+            "plain_per_request_peak": plain_peak, "plain_at_half_its_peak": plain_half,
+            "served_at_same_load": served_half,
+            "served_over_plain_mops": round(peak["mops"] / plain_peak["mops"], 2)}
 
 
 def run_reference(args, rank):

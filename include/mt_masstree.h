@@ -172,7 +172,7 @@ typedef struct mt_serve_plan {
   const uint64_t* arrival_ns;  /* arrival time after the start of the run */
   uint32_t num_requests;
   uint32_t mode;               /* MT_SERVE_SERVED or MT_SERVE_PLAIN */
-  uint32_t chunk_ops;          /* ops per device work item (0 = 32) */
+  uint32_t chunk_ops;          /* ops per device work item (0 = chosen per request from the backlog) */
   uint32_t epoch_us;           /* device time per launch of the serving loop (0 = 20000) */
   float memory_budget;         /* admit while slabs in use stay under this share of the pool (0 = 0.9) */
   uint32_t reserved;

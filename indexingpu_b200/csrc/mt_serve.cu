@@ -291,7 +291,13 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     total_ops = std::max<uint64_t>(total_ops, (uint64_t)plan->request_first_op[r] + plan->request_num_ops[r]);
   }
   if (total_ops > 0xFFFFFFFFull) return MT_ERR_INVALID_ARG;
-  const uint32_t chunk = std::max<uint32_t>(1u, std::min<uint32_t>(plan->chunk_ops ? plan->chunk_ops : 32u, 4096u));
+  // Work-item size: fixed, or (chunk_ops == 0) chosen per request from the
+  // backlog, from one op per tile of a warp while the device has idle tiles
+  // (lowest latency) up to eight per tile under load (fewer items per op).
+  const uint32_t tiles_per_warp = 32u / t->tile_size;
+  const bool auto_chunk = plan->chunk_ops == 0;
+  const uint32_t fixed_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(plan->chunk_ops, 4096u));
+  const uint32_t min_chunk = auto_chunk ? tiles_per_warp : fixed_chunk;
   const double budget = plan->memory_budget > 0.f ? plan->memory_budget : 0.9;
   mt_stats_t st{};
   int rc = mt_stats(t, &st);
@@ -354,13 +360,9 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     }
   } else {
     // Device-resident loop.
-    uint64_t total_items = 0;
-    std::vector<uint32_t> items(nreq);
-    for (uint32_t r = 0; r < nreq; ++r) {
-      items[r] = (plan->request_num_ops[r] + chunk - 1) / chunk;
-      if (items[r] == 0) items[r] = 1;
-      total_items += items[r];
-    }
+    uint64_t total_items = 0;  // ring capacity: every request cut at the smallest item size
+    for (uint32_t r = 0; r < nreq; ++r)
+      total_items += std::max<uint32_t>(1u, (plan->request_num_ops[r] + min_chunk - 1) / min_chunk);
     serve_item* d_ring = nullptr;
     unsigned long long* d_pub = nullptr;
     uint32_t *d_stop = nullptr, *d_done = nullptr, *d_finished = nullptr;
@@ -404,6 +406,10 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
       t0 = clk::now();
       std::atomic<uint32_t> completed{0};
       std::atomic<uint64_t> completed_demand{0};
+      std::atomic<uint64_t> completed_ops{0};
+      uint64_t admitted_ops = 0;
+      const uint64_t total_tiles = nwarps * tiles_per_warp;
+      uint32_t waiting_for = ~0u;
       std::atomic<bool> poll_stop{false};
       uint64_t admitted_demand = 0;
       std::vector<uint64_t> enq_completed;  // completed_demand when each epoch was enqueued
@@ -422,6 +428,7 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
             if (__atomic_load_n(&done[q], __ATOMIC_ACQUIRE)) {
               completion[q] = now_ns(t0);
               completed_demand.fetch_add(demand[q]);
+              completed_ops.fetch_add(plan->request_num_ops[q]);
               completed.fetch_add(1);
               pending[i] = pending.back();
               pending.pop_back();
@@ -458,15 +465,25 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
         const uint64_t now = now_ns(t0);
         while (r < nreq && plan->arrival_ns[r] <= now) {
           if (slabs_in_use + demand[r] > slab_budget) {
-            ++rejected_waits;  // admission waits for memory (reclaimed between launches)
+            // Admission waits for memory (slabs come back between launches).
+            if (waiting_for != r) { ++rejected_waits; waiting_for = r; }
             break;
           }
           arrival[r] = plan->arrival_ns[r];
+          uint32_t chunk = fixed_chunk;
+          if (auto_chunk) {
+            const uint64_t backlog = admitted_ops - std::min(admitted_ops, completed_ops.load());
+            const uint64_t per_tile = backlog / total_tiles;
+            chunk = tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
+          }
+          const uint32_t nops = plan->request_num_ops[r];
+          const uint32_t n_items = std::max<uint32_t>(1u, (nops + chunk - 1) / chunk);
+          admitted_ops += nops;
           uint32_t f = plan->request_first_op[r];
-          uint32_t left = plan->request_num_ops[r];
-          for (uint32_t k = 0; k < items[r]; ++k) {
+          uint32_t left = nops;
+          for (uint32_t k = 0; k < n_items; ++k) {
             const uint32_t c = std::min(left, chunk);
-            ring[published % sv.ring_cap] = serve_item{r, f, c, items[r]};
+            ring[published % sv.ring_cap] = serve_item{r, f, c, n_items};
             ++published;
             f += c;
             left -= c;
@@ -513,13 +530,13 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     if (d_ctl) cudaFree(d_ctl);
     if (d_held) cudaFree(d_held);
   }
-  const uint64_t end = now_ns(t0);
   cudaStreamSynchronize(s);
   cudaStreamDestroy(s);
-  uint64_t ops_done = 0;
+  uint64_t ops_done = 0, end = 0;
   for (uint32_t r = 0; r < nreq; ++r) {
     latency_ns[r] = completion[r] ? completion[r] - arrival[r] : 0ull;
     if (completion[r]) ops_done += plan->request_num_ops[r];
+    end = std::max<uint64_t>(end, completion[r]);
   }
   if (stats) {
     stats->wall_ns = end;

@@ -240,19 +240,34 @@ def c3(n_keys, n_queries, seed=0xC3):
 
 # ---- C5 (serving) ---------------------------------------------------------------
 
+def keys_threaded(c2, ids, threads=16):
+    """c2.keys over chunks of ids in a thread pool (numpy releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    ids = np.asarray(ids, dtype=np.int64)
+    n_chunks = max(1, min(threads, len(ids) // 65536))
+    if n_chunks == 1:
+        return c2.keys(ids)
+    with ThreadPoolExecutor(n_chunks) as ex:
+        parts = list(ex.map(c2.keys, np.array_split(ids, n_chunks)))
+    return tuple(np.concatenate([p[i] for p in parts]) for i in range(4))
+
+
 def serve_stream(c2, n_requests, rate_per_s=None, min_ops=1, max_ops=64, seed=0xC5, disjoint=False,
-                 mix=(0.5, 0.3, 0.1, 0.1), first_fresh=None):
+                 mix=(0.5, 0.3, 0.1, 0.1), first_fresh=None, op_seed=None, threads=16):
     """Open-loop request stream over a C2 tree of c2.n_preload keys.
 
-    Request r holds 1 + floor(log-uniform) ops in [min_ops, max_ops] of the C2
-    mix; arrivals are a Poisson process of rate_per_s requests per second
+    Request r holds a log-uniform number of ops in [min_ops, max_ops] of the
+    C2 mix; arrivals are a Poisson process of rate_per_s requests per second
     (None: all at time 0).  disjoint=True draws find/update/erase keys without
     replacement from the preloaded ids (and half the finds from absent ids), so
     no two ops of the whole stream touch the same key and every op's result is
     independent of how requests interleave; otherwise they are Zipf(theta) as
     in c2 batches.  Inserts always use fresh ids (from first_fresh, default
-    just above any c2.batch id range).  Returns op arrays (types, ids, keys,
-    lens, vals, vlens) and per-request first, nops, arrival_ns."""
+    the middle of c2's id space, above the ids of its batches).  Sizes and
+    arrivals follow `seed`, the ops `op_seed` (default: seed), so streams of
+    equal shape and different content can be drawn.  Returns op arrays (types,
+    ids, keys, lens, vals, vlens) and per-request first, nops, arrival_ns."""
+    os_ = seed if op_seed is None else op_seed
     r = np.arange(n_requests, dtype=np.int64)
     u = uniform01(seed, 1, r)
     lo, hi = np.log(min_ops), np.log(max_ops + 1)
@@ -261,7 +276,7 @@ def serve_stream(c2, n_requests, rate_per_s=None, min_ops=1, max_ops=64, seed=0x
     total = int(nops.sum(dtype=np.int64))
     idx = np.arange(total, dtype=np.int64)
     cum = np.cumsum(np.asarray(mix, np.float64))
-    v = uniform01(seed, 2, idx)
+    v = uniform01(os_, 2, idx)
     types = np.where(v < cum[0], REQ_FIND, np.where(v < cum[1], REQ_INSERT,
                                                     np.where(v < cum[2], REQ_UPDATE, REQ_ERASE))).astype(np.uint8)
     if first_fresh is None:
@@ -272,12 +287,12 @@ def serve_stream(c2, n_requests, rate_per_s=None, min_ops=1, max_ops=64, seed=0x
     if disjoint:
         if total > c2.n_preload:
             raise ValueError("disjoint stream needs at least as many preloaded keys as ops")
-        old = feistel_permute(idx.astype(U64), c2.n_preload, seed).astype(np.int64)
-        miss = (types == REQ_FIND) & (rnd32(seed, 3, idx) & np.uint32(1)).astype(bool)
+        old = feistel_permute(idx.astype(U64), c2.n_preload, os_).astype(np.int64)
+        miss = (types == REQ_FIND) & (rnd32(os_, 3, idx) & np.uint32(1)).astype(bool)
         ids = np.where((types == REQ_INSERT) | miss, fresh, old)
     else:
-        ids = np.where(types == REQ_INSERT, fresh, zipf_sample(c2.n_preload, c2.theta, uniform01(seed, 4, idx)))
-    keys, lens, vals, vlens = c2.keys(ids)
+        ids = np.where(types == REQ_INSERT, fresh, zipf_sample(c2.n_preload, c2.theta, uniform01(os_, 4, idx)))
+    keys, lens, vals, vlens = keys_threaded(c2, ids, threads)
     upd = types == REQ_UPDATE
     with np.errstate(over="ignore"):
         newv = (vals.astype(U64) ^ U64(0x5BD1E995)).astype(np.uint32)
