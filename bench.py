@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
+    ap.add_argument("--pool-gb", type=float, default=0.0,
+                    help="slab pool size in GB (default: 60%% of the free device memory)")
     ap.add_argument("--sections", default="batched,served",
                     help="extra measurements at N=1: batched (256 sub-batches, tuned persistent launch from a "
                          "CUDA graph, against one call per sub-batch), served (request loop over 64M keys, "
@@ -207,7 +209,10 @@ def run_ours(args, rank, world, dist):
     e2e_w, e2e_k = 2, max(1, min(args.e2e_steps, args.steps))
     e2e_batches = gen_batches(c2, nb, e2e_w + e2e_k, args.batch)
 
-    tree = GpuMasstree(pool_ratio=0.6, tile_size=args.tile)
+    if args.pool_gb > 0:
+        tree = GpuMasstree(pool_bytes=int(args.pool_gb * (1 << 30)), tile_size=args.tile)
+    else:
+        tree = GpuMasstree(pool_ratio=0.6, tile_size=args.tile)
     tree.set_write_tile_size(args.write_tile)
     if args.blocks_per_sm:
         tree.set_blocks_per_sm(args.blocks_per_sm)
