@@ -290,7 +290,6 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   if (n <= t->split_cap) return MT_OK;
   if (cudaStreamSynchronize(s) != cudaSuccess) return MT_ERR_CUDA;
   if (t->split_idx) cudaFree(t->split_idx);
-  if (t->batches_mem) cudaFree(t->batches_mem);
   t->split_idx = nullptr;
   t->split_cap = 0;
   // [counts(32 words, one line)] [find indices n] [insert indices n] [update/erase indices n]
@@ -360,13 +359,33 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   u.index = upderase_idx;
   u.n_dev = counts + 2;
   if (a.n >= kClassBarrierMin) {
-    // Large batch: one launch per class.
-    rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, s);
-    if (rc) return rc;
+    // Large batch: one launch per class, each compiled for its class only.
+    // The classes of one mixed batch have no order among each other, so they
+    // go to three streams (the caller's and two of the tree's, forked and
+    // joined by events): the blocks of one class fill the SMs that another
+    // class's tail leaves idle.
+    if (!t->ev_fork) {
+      bool ok = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+      for (int k = 0; k < 2 && ok; ++k)
+        ok = cudaStreamCreateWithFlags(&t->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&t->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
+      if (!ok) return MT_ERR_CUDA;
+    }
+    if (cudaEventRecord(t->ev_fork, s) != cudaSuccess) return MT_ERR_CUDA;
+    for (int k = 0; k < 2; ++k)
+      if (cudaStreamWaitEvent(t->side[k], t->ev_fork, 0) != cudaSuccess) return MT_ERR_CUDA;
     const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
     rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
-    if (rc) return rc;
-    return launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, s);
+    if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
+    if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, t->side[1]);
+    // Join even after an error, so that the side streams never run ahead of
+    // the caller's stream.
+    for (int k = 0; k < 2; ++k) {
+      if (cudaEventRecord(t->ev_join[k], t->side[k]) != cudaSuccess ||
+          cudaStreamWaitEvent(s, t->ev_join[k], 0) != cudaSuccess)
+        rc = rc ? rc : MT_ERR_CUDA;
+    }
+    return rc;
   }
   switch (t->tile_size) {
     case 4: return launch_mixed_classes_tf<4>(t, f, i, u, s);
@@ -485,8 +504,14 @@ int mt_destroy(mt_masstree* t) {
   cudaDeviceSynchronize();
   if (t->frames) cudaFree(t->frames);
   if (t->split_idx) cudaFree(t->split_idx);
+  if (t->batches_mem) cudaFree(t->batches_mem);
   if (t->mem) cudaFree(t->mem);
   if (t->h_err) cudaFreeHost(t->h_err);
+  for (int k = 0; k < 2; ++k) {
+    if (t->side[k]) cudaStreamDestroy(t->side[k]);
+    if (t->ev_join[k]) cudaEventDestroy(t->ev_join[k]);
+  }
+  if (t->ev_fork) cudaEventDestroy(t->ev_fork);
   delete t;
   return MT_OK;
 }

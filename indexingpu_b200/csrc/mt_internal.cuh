@@ -169,6 +169,11 @@ struct mt_masstree {
   uint32_t blocks_per_sm = 0;    // 0 = occupancy limit
   uint32_t* split_idx = nullptr; // mixed-batch partition scratch
   uint32_t split_cap = 0;
+  // Streams and events of the forked class launches of large mixed batches
+  // (created on first use).
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[2] = {nullptr, nullptr};
   void* mem = nullptr;
   mtb::tree_view tv{};
   mtb::scan_frame* frames = nullptr;
