@@ -44,15 +44,17 @@ def time_trial(tree, case, config, stream):
 
 
 def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_TILES, bucketing=BUCKETING,
-         blocks_per_sm=BLOCKS_PER_SM, log=None):
+         blocks_per_sm=BLOCKS_PER_SM, log=None, trial=time_trial):
     """Coordinate-descent search; returns (best config, list of trials).
 
     make_case(i) (i = 0 for the warm-up, then 1, 2, ...) returns a dict with
     keys descriptors (device tensor of mt_subbatch records), num_subbatches,
     total, max_key_length, max_value_length (and anything that must stay
-    alive while it runs)."""
-    import torch
-    stream = stream or torch.cuda.current_stream()
+    alive while it runs).  trial(tree, case, config, stream) -> Mops/s runs
+    one measurement (time_trial by default)."""
+    if stream is None and trial is time_trial:
+        import torch
+        stream = torch.cuda.current_stream()
     trials = []
     t_start = time.time()
 
@@ -62,11 +64,11 @@ def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_
     warm = make_case(0)
     for ft in find_tiles:
         for wt in write_tiles:
-            time_trial(tree, warm, dict(find_tile=ft, write_tile=wt, bucketing=False, blocks_per_sm=0), stream)
+            trial(tree, warm, dict(find_tile=ft, write_tile=wt, bucketing=False, blocks_per_sm=0), stream)
     del warm
 
     def run(config):
-        mops = time_trial(tree, make_case(len(trials) + 1), config, stream)
+        mops = trial(tree, make_case(len(trials) + 1), config, stream)
         trials.append(dict(config, mops=round(mops, 2)))
         if log:
             log(trials[-1])

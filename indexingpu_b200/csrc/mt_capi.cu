@@ -298,45 +298,6 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   return MT_OK;
 }
 
-// Partitioned mixed batch: the classes of one batch in one launch.
-template <int TF, int TW>
-__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) mixed_classes_kernel(tree_view tv, batch_args f,
-                                                                                     batch_args i, batch_args u) {
-  slab_cache<TW> wcache;
-  wcache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / TW);
-  serve_mixed_classes<TF, TW>(tv, wcache, f, i, u);
-  tile<TW> tw;
-  wcache.release(tw, tv.pool);
-}
-
-template <int TF, int TW>
-int launch_mixed_classes(mt_masstree* t, const batch_args& f, const batch_args& i, const batch_args& u,
-                         cudaStream_t s) {
-  const void* fn = (const void*)mixed_classes_kernel<TF, TW>;
-  const int grid = grid_for(t, fn);
-  mixed_classes_kernel<TF, TW><<<grid, kBlock, 0, s>>>(t->tv, f, i, u);
-  return cuda_status(cudaGetLastError());
-}
-
-// Mixed batches serve writes with 16- or 32-lane tiles (narrower write tiles,
-// allowed for plain insert/update/erase calls, are widened to 16 here).
-template <int TF>
-int launch_mixed_classes_tf(mt_masstree* t, const batch_args& f, const batch_args& i, const batch_args& u,
-                            cudaStream_t s) {
-  switch (t->write_tile_size <= 16 ? 16u : 32u) {
-    case 16: return launch_mixed_classes<TF, 16>(t, f, i, u, s);
-    case 32: return launch_mixed_classes<TF, 32>(t, f, i, u, s);
-    default: return MT_ERR_INVALID_ARG;
-  }
-}
-
-// A mixed batch: reclaim, partition by class (finds, inserts, updates+erases),
-// then either one launch in which every tile serves finds with the find tile
-// width, then inserts, then updates and erases with the write tile width
-// (small batches), or one launch per class (large batches).  Requests of one mixed batch have no defined order, so
-// class by class is one of the orders the reference allows; it removes the
-// divergence between the tiles of a warp and keeps the code each warp runs at
-// a time small.
 int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   if (a.n == 0) return MT_OK;
   int rc = ensure_split_scratch(t, a.n, s);
@@ -358,42 +319,35 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   i.n_dev = counts + 1;
   u.index = upderase_idx;
   u.n_dev = counts + 2;
-  if (a.n >= kClassBarrierMin) {
-    // Large batch: one launch per class, each compiled for its class only.
-    // The classes of one mixed batch have no order among each other, so they
-    // go to three streams (the caller's and two of the tree's, forked and
-    // joined by events): the blocks of one class fill the SMs that another
-    // class's tail leaves idle.
-    if (!t->ev_fork) {
-      bool ok = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming) == cudaSuccess;
-      for (int k = 0; k < 2 && ok; ++k)
-        ok = cudaStreamCreateWithFlags(&t->side[k], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&t->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
-      if (!ok) return MT_ERR_CUDA;
-    }
-    if (cudaEventRecord(t->ev_fork, s) != cudaSuccess) return MT_ERR_CUDA;
-    for (int k = 0; k < 2; ++k)
-      if (cudaStreamWaitEvent(t->side[k], t->ev_fork, 0) != cudaSuccess) return MT_ERR_CUDA;
-    const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
-    rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
-    if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
-    if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, t->side[1]);
-    // Join even after an error, so that the side streams never run ahead of
-    // the caller's stream.
-    for (int k = 0; k < 2; ++k) {
-      if (cudaEventRecord(t->ev_join[k], t->side[k]) != cudaSuccess ||
-          cudaStreamWaitEvent(s, t->ev_join[k], 0) != cudaSuccess)
-        rc = rc ? rc : MT_ERR_CUDA;
-    }
-    return rc;
+  // One launch per class, each compiled for its class only.
+  // The classes of one mixed batch have no order among each other, so they
+  // go to three streams (the caller's and two of the tree's, forked and
+  // joined by events): the blocks of one class fill the SMs that another
+  // class's tail leaves idle.
+  if (!t->ev_fork) {
+    bool ok = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < 2 && ok; ++k)
+      ok = cudaStreamCreateWithFlags(&t->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&t->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return MT_ERR_CUDA;
   }
-  switch (t->tile_size) {
-    case 4: return launch_mixed_classes_tf<4>(t, f, i, u, s);
-    case 8: return launch_mixed_classes_tf<8>(t, f, i, u, s);
-    case 16: return launch_mixed_classes_tf<16>(t, f, i, u, s);
-    case 32: return launch_mixed_classes_tf<32>(t, f, i, u, s);
-    default: return MT_ERR_INVALID_ARG;
+  if (cudaEventRecord(t->ev_fork, s) != cudaSuccess) return MT_ERR_CUDA;
+  for (int k = 0; k < 2; ++k)
+    if (cudaStreamWaitEvent(t->side[k], t->ev_fork, 0) != cudaSuccess) return MT_ERR_CUDA;
+  // Write classes run with 16- or 32-lane tiles (narrower write tiles, allowed
+  // for plain insert/update/erase calls, are widened to 16 here).
+  const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
+  rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
+  if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
+  if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, t->side[1]);
+  // Join even after an error, so that the side streams never run ahead of
+  // the caller's stream.
+  for (int k = 0; k < 2; ++k) {
+    if (cudaEventRecord(t->ev_join[k], t->side[k]) != cudaSuccess ||
+        cudaStreamWaitEvent(s, t->ev_join[k], 0) != cudaSuccess)
+      rc = rc ? rc : MT_ERR_CUDA;
   }
+  return rc;
 }
 
 template <int T, bool CONC>

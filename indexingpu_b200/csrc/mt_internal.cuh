@@ -10,9 +10,10 @@ namespace mtb {
 constexpr int kBlock = 128;
 constexpr uint32_t kShards = 64;
 constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
-// Mixed batches of at least this many requests serve their classes one after
-// the other (all warps in the same code at a time, measured faster on 1M
-// batches); smaller ones let tiles flow from class to class (no class tail).
+// In the persistent launch of mt_mixed_batches, sub-batches of at least this
+// many requests serve their classes one after the other with a grid barrier
+// between them (all warps in the same code at a time, faster on large
+// sub-batches); smaller ones let tiles flow from class to class.
 constexpr uint32_t kClassBarrierMin = 1u << 17;
 
 #ifndef MT_MIN_BLOCKS_PER_SM

@@ -166,3 +166,39 @@ def test_mixed_batches_graph_replay():
     finally:
         ref.close()
         new.close()
+
+
+def test_autotune_small_cases():
+    """The autotuner runs every trial through mt_mixed_batches on fresh cases,
+    returns a configuration from its grid, and leaves a valid tree."""
+    import torch
+    from indexingpu_b200 import GpuMasstree, autotune
+    c2 = wl.C2(n_preload=20000, n_prefixes=64)
+    keys, lens, vals, vlens = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in c2.keys(np.arange(20000)))
+    t = GpuMasstree(pool_bytes=512 << 20, tile_size=8)
+    try:
+        t.insert(keys, MAXK, lens, vals, MAXV, vlens, 20000)
+        t.sync()
+
+        def make_case(i):
+            st = wl.serve_stream(c2, 4, min_ops=64, max_ops=4096, seed=11, op_seed=100 + i,
+                                 first_fresh=(1 << 20) + i * (1 << 16))
+            d = {k: torch.from_numpy(np.ascontiguousarray(st[k])).cuda() for k in ("types", "keys", "lens", "vals",
+                                                                                    "vlens")}
+            res = torch.zeros(len(st["types"]), dtype=torch.bool, device="cuda")
+            subs = []
+            for f, n in zip(st["first"].tolist(), st["nops"].tolist()):
+                subs.append(dict(types=d["types"][f:f + n], keys=d["keys"][f:f + n], lens=d["lens"][f:f + n],
+                                 vals=d["vals"][f:f + n], vlens=d["vlens"][f:f + n], results=res[f:f + n], n=n))
+            desc = torch.from_numpy(pack_subbatches(subs)).cuda()
+            return dict(descriptors=desc, num_subbatches=len(subs), total=int(st["nops"].sum()),
+                        max_key_length=MAXK, max_value_length=MAXV, keep=(d, res))
+
+        best, trials = autotune.tune(t, make_case, blocks_per_sm=(2, 8))
+        assert len(trials) == 16 + 2
+        assert best["find_tile"] in autotune.FIND_TILES and best["write_tile"] in autotune.WRITE_TILES
+        assert all(tr["mops"] > 0 for tr in trials)
+        ok, _, report = t.validate()
+        assert ok, report
+    finally:
+        t.close()
