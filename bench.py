@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--tile", type=int, default=8, help="lanes per find")
     ap.add_argument("--write-tile", type=int, default=32, help="lanes per insert/update/erase")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--bucket", type=int, default=0, help="1: mixed_batch serves short keys before long keys")
     ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
@@ -235,7 +236,7 @@ def run_ours(args, rank, world, dist):
 
     def step(b):
         tree.mixed_batch(b["types"], b["keys"], MAXK, b["lens"], b["vals"], MAXV, b["vlens"], b["res"], args.batch,
-                         stream=stream)
+                         stream=stream, bucket_keys=bool(args.bucket))
 
     for i in range(args.warmup):
         step(dev_b[i])
@@ -290,7 +291,7 @@ def run_ours(args, rank, world, dist):
         for k in ("types", "keys", "lens", "vals", "vlens"):
             dbuf[k].copy_(h[k], non_blocking=True)
         tree.mixed_batch(dbuf["types"], dbuf["keys"], MAXK, dbuf["lens"], dbuf["vals"], MAXV, dbuf["vlens"],
-                         dbuf["res"], args.batch, stream=stream)
+                         dbuf["res"], args.batch, stream=stream, bucket_keys=bool(args.bucket))
         for k in ("vals", "vlens", "res"):
             out[k].copy_(dbuf[k], non_blocking=True)
 
@@ -420,7 +421,7 @@ def run_batched(args, tree, c2, stream):
     e0.record(stream)
     for sb in _subbatches(dev, st):
         tree.mixed_batch(sb["types"], sb["keys"], MAXK, sb["lens"], sb["vals"], MAXV, sb["vlens"], sb["results"],
-                         sb["n"], stream=stream)
+                         sb["n"], stream=stream, bucket_keys=bool(args.bucket))
     e1.record(stream)
     tree.sync(stream)
     per_call = total / (e0.elapsed_time(e1) / 1e3) / 1e6
@@ -448,7 +449,8 @@ def run_batched(args, tree, c2, stream):
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=side):
-        tree.mixed_batches(desc, args.subbatches, MAXK, MAXV, stream=side, bucket_keys=best["bucketing"])
+        tree.mixed_batches(desc, args.subbatches, MAXK, MAXV, stream=side, bucket_keys=best["bucketing"],
+                           persistent=best["form"] == "persistent")
     torch.cuda.synchronize()
     with torch.cuda.stream(side):
         e0.record(side)

@@ -50,8 +50,10 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
 #define MT_FLAG_USE_UPPER_KEY 4u    /* scan stops after upper_keys (reference `use_upper_key`) */
 #define MT_FLAG_SINGLE_PASS 8u      /* mixed_batch: one kernel for every kind instead of
                                        finds-then-writes passes (comparison switch) */
-#define MT_FLAG_BUCKET_KEYS 16u     /* mixed_batches: serve short keys before long keys in
+#define MT_FLAG_BUCKET_KEYS 16u     /* mixed_batch(es): serve short keys before long keys in
                                        every request class */
+#define MT_FLAG_PERSISTENT 32u      /* mixed_batches: one cooperative persistent launch for all
+                                       sub-batches instead of three class kernels per sub-batch */
 
 /* One sub-batch of mt_mixed_batches: the buffers of one mt_mixed_batch call
  * (device pointers; max lengths are common to all sub-batches). */
@@ -140,12 +142,17 @@ int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32
 int mt_batches_reserve(mt_masstree* tree, uint32_t max_subbatches, uint64_t max_total_requests);
 
 /* Serve num_subbatches mixed batches in order, with the results of one
- * mt_mixed_batch call per sub-batch, in one persistent cooperative launch
- * (plus a partition pass): sub-batch k+1 sees every effect of sub-batch k.
- * `subbatches` is a DEVICE array of descriptors; nothing is read back to the
- * host, so the call can be captured in a CUDA graph and replayed after the
- * descriptors' contents change.  Needs mt_batches_reserve; flags may hold
- * MT_FLAG_BUCKET_KEYS.  Find tile width: mt_set_tile_size (4/8/16/32); write
+ * mt_mixed_batch call per sub-batch: sub-batch k+1 sees every effect of
+ * sub-batch k.  One partition pass files every request of every sub-batch
+ * under its class; then, by default, each sub-batch runs its three class
+ * kernels side by side on forked streams (3 launches per sub-batch), or, with
+ * MT_FLAG_PERSISTENT, one cooperative persistent launch serves all
+ * sub-batches with a grid barrier between them.  `subbatches` is a DEVICE
+ * array of descriptors; nothing is read back to the host and the number of
+ * launches depends only on num_subbatches, so the call can be captured in a
+ * CUDA graph and replayed after the descriptors' contents change.  Needs
+ * mt_batches_reserve; flags may hold MT_FLAG_BUCKET_KEYS and
+ * MT_FLAG_PERSISTENT.  Find tile width: mt_set_tile_size (4/8/16/32); write
  * tile width: mt_set_write_tile_size (16 or 32).  The batched counterpart of
  * the reference's per-call mixed_batch (gpu_masstree.hpp:173-191). */
 int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t num_subbatches,

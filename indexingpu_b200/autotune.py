@@ -1,12 +1,14 @@
 """Autotuner for the batched form (mt_mixed_batches).
 
-Searches the launch shape of the persistent launch over
-  find tile (lanes per find: 4, 8, 16, 32) x write tile (lanes per insert,
-  update and erase: 16, 32) x key-length bucketing (off, on),
+Searches the form and launch shape of the call over
+  form (three class kernels per sub-batch on forked streams, or one
+  persistent launch for all sub-batches) x find tile (lanes per find: 4, 8,
+  16, 32) x write tile (lanes per insert, update and erase: 16, 32) x
+  key-length bucketing (off, on),
 then, for the best of those, blocks per SM 1..8.  This is coordinate descent
-(16 + 8 trials rather than the 128 points of the full grid): blocks per SM only
-trades occupancy against per-warp registers, and is measured with the tile
-choice fixed.
+(32 + 8 trials rather than the 256 points of the full grid): blocks per SM only
+trades occupancy against per-warp registers, and is measured with the other
+choices fixed.
 
 Every trial runs on a fresh case from `make_case(i)`: the tree changes under
 every trial (inserts add keys, erases remove them), so replaying one case would
@@ -18,6 +20,7 @@ import time
 FIND_TILES = (4, 8, 16, 32)
 WRITE_TILES = (16, 32)
 BUCKETING = (False, True)
+FORMS = ("forked", "persistent")
 BLOCKS_PER_SM = tuple(range(1, 9))
 
 
@@ -37,14 +40,15 @@ def time_trial(tree, case, config, stream):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     tree.mixed_batches(case["descriptors"], case["num_subbatches"], case["max_key_length"],
-                       case["max_value_length"], stream=stream, bucket_keys=config["bucketing"])
+                       case["max_value_length"], stream=stream, bucket_keys=config["bucketing"],
+                       persistent=config.get("form") == "persistent")
     e1.record(stream)
     tree.sync(stream)
     return case["total"] / (e0.elapsed_time(e1) / 1e3) / 1e6
 
 
 def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_TILES, bucketing=BUCKETING,
-         blocks_per_sm=BLOCKS_PER_SM, log=None, trial=time_trial):
+         blocks_per_sm=BLOCKS_PER_SM, log=None, trial=time_trial, forms=FORMS):
     """Coordinate-descent search; returns (best config, list of trials).
 
     make_case(i) (i = 0 for the warm-up, then 1, 2, ...) returns a dict with
@@ -62,9 +66,11 @@ def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_
     # loading and first-call set-up would otherwise land in the first trials);
     # one case serves them all.
     warm = make_case(0)
-    for ft in find_tiles:
-        for wt in write_tiles:
-            trial(tree, warm, dict(find_tile=ft, write_tile=wt, bucketing=False, blocks_per_sm=0), stream)
+    for fm in forms:
+        for ft in find_tiles:
+            for wt in write_tiles:
+                trial(tree, warm, dict(form=fm, find_tile=ft, write_tile=wt, bucketing=False, blocks_per_sm=0),
+                      stream)
     del warm
 
     def run(config):
@@ -75,13 +81,14 @@ def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_
         return mops
 
     best, best_mops = None, -1.0
-    for ft in find_tiles:
-        for wt in write_tiles:
-            for bk in bucketing:
-                cfg = dict(find_tile=ft, write_tile=wt, bucketing=bk, blocks_per_sm=0)
-                m = run(cfg)
-                if m > best_mops:
-                    best, best_mops = cfg, m
+    for fm in forms:
+        for ft in find_tiles:
+            for wt in write_tiles:
+                for bk in bucketing:
+                    cfg = dict(form=fm, find_tile=ft, write_tile=wt, bucketing=bk, blocks_per_sm=0)
+                    m = run(cfg)
+                    if m > best_mops:
+                        best, best_mops = cfg, m
     for b in blocks_per_sm:
         cfg = dict(best, blocks_per_sm=b)
         m = run(cfg)

@@ -1,23 +1,25 @@
-// Many mixed sub-batches in one persistent launch (mt_mixed_batches).
+// Many mixed sub-batches in one call (mt_mixed_batches).
 //
 // The reference serves one host call per batch (include/kernels.hpp:81-103):
-// each call pays host launch overhead, an occupancy query and the tail of its
-// slowest request.  Here a list of sub-batches (device descriptors) is served
-// by three launches whatever its length:
+// each call pays host launch overhead, an occupancy query, a partition pass
+// and the tail of its slowest request.  Here a list of sub-batches (device
+// descriptors) is served by
 //   1. batches_prepare_kernel: prefix sums of the sub-batch sizes, counters reset;
 //   2. batches_partition_kernel: every request of every sub-batch is filed
 //      under (sub-batch, class) with class = find / insert / update+erase,
 //      optionally split into short and long keys (filled from the two ends of
 //      the class's index region, so each class is served short keys first);
-//   3. batches_persistent_kernel: a cooperative grid walks the sub-batches in
-//      order with one grid barrier between sub-batches; inside a sub-batch the
-//      tiles flow from finds to inserts to updates and erases without one.
+//   3. either (default) for every sub-batch its three batches_class_kernel
+//      launches side by side on forked streams, joined before the next
+//      sub-batch, or (MT_FLAG_PERSISTENT) batches_persistent_kernel: a
+//      cooperative grid walks the sub-batches in order with one grid barrier
+//      between sub-batches.
 // Sub-batch k+1 observes every effect of sub-batch k, as with one host call per
-// sub-batch; inside a sub-batch the classes run finds, inserts, then updates
-// and erases (one of the orders a mixed batch allows).  Nothing in the call
-// allocates once mt_batches_reserve has sized the scratch, and no host value
-// depends on the sub-batch contents, so the call can be captured in a CUDA
-// graph and replayed with new descriptor contents.
+// sub-batch; inside a sub-batch the classes have no order among each other
+// (as inside one mixed batch).  Nothing in the call allocates once
+// mt_batches_reserve has sized the scratch, and no host value depends on the
+// sub-batch contents, so the call can be captured in a CUDA graph and replayed
+// with new descriptor contents.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -158,11 +160,63 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_persiste
   wcache.release(tw, tv.pool);
 }
 
+// One class of one sub-batch (the forked form): the class kernels of a
+// sub-batch run side by side, each compiled for its class only.
+template <int T, int OP>
+__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_class_kernel(tree_view tv, batches_view b,
+                                                                                     uint32_t sb) {
+  if (b.status[0]) return;
+  constexpr uint32_t cls = OP == OP_FIND ? 0u : (OP == OP_PASS_INSERT ? 1u : 2u);
+  tile<T> t;
+  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
+  const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
+  slab_cache<T> cache;
+  cache.init(tv.pool, tile_id);
+  serve_requests<T, OP, true>(t, tv, cache, class_args(b, sb, cls), tile_id, num_tiles);
+  cache.release(t, tv.pool);
+}
+
 }  // namespace mtb
 
 using namespace mtb;
 
 namespace {
+
+template <int T, int OP>
+int launch_class(mt_masstree* t, const batches_view& b, uint32_t sb, cudaStream_t s) {
+  const void* fn = (const void*)batches_class_kernel<T, OP>;
+  int bps = host_max_blocks_per_sm(fn, kBlock, 0);
+  if (t->blocks_per_sm > 0) bps = std::min<int>(bps, (int)t->blocks_per_sm);
+  batches_class_kernel<T, OP><<<std::max(bps, 1) * t->sms, kBlock, 0, s>>>(t->tv, b, sb);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
+}
+
+template <int OP>
+int launch_class_tile(mt_masstree* t, uint32_t tile, const batches_view& b, uint32_t sb, cudaStream_t s) {
+  switch (tile) {
+    case 4: return launch_class<4, OP>(t, b, sb, s);
+    case 8: return launch_class<8, OP>(t, b, sb, s);
+    case 16: return launch_class<16, OP>(t, b, sb, s);
+    default: return launch_class<32, OP>(t, b, sb, s);
+  }
+}
+
+// Forked form: per sub-batch, the insert class on the caller's stream and the
+// find and update/erase classes on the tree's two side streams, joined before
+// the next sub-batch starts.
+int launch_forked(mt_masstree* t, const batches_view& b, cudaStream_t s) {
+  const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
+  for (uint32_t sb = 0; sb < b.nsub; ++sb) {
+    int rc = host_fork(t, s);
+    if (rc) return rc;
+    rc = launch_class_tile<OP_PASS_INSERT>(t, tw, b, sb, s);
+    if (!rc) rc = launch_class_tile<OP_FIND>(t, t->tile_size, b, sb, t->side[0]);
+    if (!rc) rc = launch_class_tile<OP_PASS_UPDERASE>(t, tw, b, sb, t->side[1]);
+    rc = host_join(t, s, rc);
+    if (rc) return rc;
+  }
+  return MT_OK;
+}
 
 template <int TF, int TW>
 int launch_persistent(mt_masstree* t, const batches_view& b, cudaStream_t s) {
@@ -238,6 +292,7 @@ extern "C" int mt_mixed_batches(mt_masstree* t, const mt_subbatch* subbatches, u
   batches_prepare_kernel<<<1, 256, 0, s>>>(b, t->tv.pool);
   batches_partition_kernel<<<t->sms * 4, 256, 0, s>>>(b);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
+  if (!(flags & MT_FLAG_PERSISTENT)) return launch_forked(t, b, s);
   switch (t->tile_size) {
     case 4: return launch_persistent_tf<4>(t, b, s);
     case 8: return launch_persistent_tf<8>(t, b, s);

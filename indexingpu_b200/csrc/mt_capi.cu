@@ -53,30 +53,37 @@ __global__ void partition_kernel(const uint8_t* types, uint32_t n, uint32_t* fin
 }
 
 // Split a mixed batch into finds, inserts and updates+erases (one atomic per
-// warp and class).  counts = {finds, inserts, updates+erases}.
-__global__ void partition3_kernel(const uint8_t* types, uint32_t n, uint32_t* find_idx, uint32_t* insert_idx,
+// warp and counter).  Each class has an index region of n entries; with
+// bucketing, keys longer than half the maximum length fill it from the back,
+// so that the tiles of a warp serve keys of similar length (similar paths)
+// side by side.  counts[2c] / counts[2c+1] = entries from the front / back of
+// class c's region (c = finds, inserts, updates+erases).
+__global__ void partition3_kernel(const uint8_t* types, const uint32_t* key_lengths, uint32_t max_key_length,
+                                  uint32_t bucket_keys, uint32_t n, uint32_t* find_idx, uint32_t* insert_idx,
                                   uint32_t* upderase_idx, uint32_t* counts) {
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n;
        base += gridDim.x * blockDim.x) {
     const uint32_t i = base + lane;
-    const uint32_t k = i < n ? types[i] : 0xFFu;
-    const uint32_t m[3] = {__ballot_sync(0xFFFFFFFFu, k == MT_REQ_FIND),
-                           __ballot_sync(0xFFFFFFFFu, k == MT_REQ_INSERT),
-                           __ballot_sync(0xFFFFFFFFu, i < n && k != MT_REQ_FIND && k != MT_REQ_INSERT)};
-    uint32_t b[3] = {0, 0, 0};
+    const bool valid = i < n;
+    const uint32_t k = valid ? types[i] : 0xFFu;
+    const uint32_t c = k == MT_REQ_FIND ? 0u : (k == MT_REQ_INSERT ? 1u : 2u);
+    uint32_t bucket = 0;
+    if (valid && bucket_keys && key_lengths) bucket = (2u * key_lengths[i] > max_key_length) ? 1u : 0u;
+    const uint32_t slot = valid ? c * 2u + bucket : 0xFFu;
+    uint32_t m[6], b[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) m[q] = __ballot_sync(0xFFFFFFFFu, slot == (uint32_t)q);
     if (lane == 0) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        if (m[c]) b[c] = atomicAdd(counts + c, (uint32_t)__popc(m[c]));
+      for (int q = 0; q < 6; ++q) b[q] = m[q] ? atomicAdd(counts + q, (uint32_t)__popc(m[q])) : 0u;
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) b[c] = __shfl_sync(0xFFFFFFFFu, b[c], 0);
-    const uint32_t below = (1u << lane) - 1u;
-    if (i < n) {
-      const int c = k == MT_REQ_FIND ? 0 : (k == MT_REQ_INSERT ? 1 : 2);
+    for (int q = 0; q < 6; ++q) b[q] = __shfl_sync(0xFFFFFFFFu, b[q], 0);
+    if (valid) {
+      const uint32_t r = reg_select(b, slot) + __popc(reg_select(m, slot) & ((1u << lane) - 1u));
       uint32_t* dst = c == 0 ? find_idx : (c == 1 ? insert_idx : upderase_idx);
-      dst[b[c] + __popc(m[c] & below)] = i;
+      dst[bucket ? n - 1u - r : r] = i;
     }
   }
 }
@@ -211,6 +218,33 @@ int host_max_blocks_per_sm(const void* fn, int block, size_t smem) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, smem) != cudaSuccess || b <= 0) b = 1;
   return b;
 }
+// Make the tree's two side streams wait for the work queued so far on s.
+int host_fork(mt_masstree* t, cudaStream_t s) {
+  if (!t->ev_fork) {
+    bool ok = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < 2 && ok; ++k)
+      ok = cudaStreamCreateWithFlags(&t->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&t->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return MT_ERR_CUDA;
+  }
+  if (cudaEventRecord(t->ev_fork, s) != cudaSuccess) return MT_ERR_CUDA;
+  for (int k = 0; k < 2; ++k)
+    if (cudaStreamWaitEvent(t->side[k], t->ev_fork, 0) != cudaSuccess) return MT_ERR_CUDA;
+  return MT_OK;
+}
+
+// Make s wait for the side streams.  Called after a fork even when a launch
+// failed (rc != MT_OK, returned unchanged), so that the side streams never run
+// ahead of the caller's stream.
+int host_join(mt_masstree* t, cudaStream_t s, int rc) {
+  for (int k = 0; k < 2; ++k) {
+    if (cudaEventRecord(t->ev_join[k], t->side[k]) != cudaSuccess ||
+        cudaStreamWaitEvent(s, t->ev_join[k], 0) != cudaSuccess)
+      rc = rc ? rc : MT_ERR_CUDA;
+  }
+  return rc;
+}
+
 int host_launch_reclaim(mt_masstree* t, cudaStream_t s) {
   reclaim_kernel<<<kShards, 256, 0, s>>>(t->tv.pool);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
@@ -298,7 +332,7 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   return MT_OK;
 }
 
-int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
+int launch_mixed_split(mt_masstree* t, batch_args a, bool bucket_keys, cudaStream_t s) {
   if (a.n == 0) return MT_OK;
   int rc = ensure_split_scratch(t, a.n, s);
   if (rc) return rc;
@@ -308,46 +342,34 @@ int launch_mixed_split(mt_masstree* t, batch_args a, cudaStream_t s) {
   uint32_t* find_idx = t->split_idx + 32;
   uint32_t* insert_idx = find_idx + a.n;
   uint32_t* upderase_idx = insert_idx + a.n;
-  if (cudaMemsetAsync(counts, 0, 3 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+  if (cudaMemsetAsync(counts, 0, 6 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
   partition3_kernel<<<std::max(1, std::min(t->sms * 8, (int)((a.n + 255) / 256))), 256, 0, s>>>(
-      a.types, a.n, find_idx, insert_idx, upderase_idx, counts);
+      a.types, a.key_lengths, a.max_key_length, bucket_keys ? 1u : 0u, a.n, find_idx, insert_idx, upderase_idx,
+      counts);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
   batch_args f = a, i = a, u = a;
-  f.index = find_idx;
-  f.n_dev = counts;
-  i.index = insert_idx;
-  i.n_dev = counts + 1;
-  u.index = upderase_idx;
-  u.n_dev = counts + 2;
+  uint32_t* idx[3] = {find_idx, insert_idx, upderase_idx};
+  batch_args* cls[3] = {&f, &i, &u};
+  for (int c = 0; c < 3; ++c) {
+    cls[c]->index = idx[c];
+    cls[c]->n_dev = counts + 2 * c;
+    cls[c]->n_back_dev = counts + 2 * c + 1;
+    cls[c]->region = a.n;
+  }
   // One launch per class, each compiled for its class only.
   // The classes of one mixed batch have no order among each other, so they
   // go to three streams (the caller's and two of the tree's, forked and
   // joined by events): the blocks of one class fill the SMs that another
   // class's tail leaves idle.
-  if (!t->ev_fork) {
-    bool ok = cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming) == cudaSuccess;
-    for (int k = 0; k < 2 && ok; ++k)
-      ok = cudaStreamCreateWithFlags(&t->side[k], cudaStreamNonBlocking) == cudaSuccess &&
-           cudaEventCreateWithFlags(&t->ev_join[k], cudaEventDisableTiming) == cudaSuccess;
-    if (!ok) return MT_ERR_CUDA;
-  }
-  if (cudaEventRecord(t->ev_fork, s) != cudaSuccess) return MT_ERR_CUDA;
-  for (int k = 0; k < 2; ++k)
-    if (cudaStreamWaitEvent(t->side[k], t->ev_fork, 0) != cudaSuccess) return MT_ERR_CUDA;
+  rc = host_fork(t, s);
+  if (rc) return rc;
   // Write classes run with 16- or 32-lane tiles (narrower write tiles, allowed
   // for plain insert/update/erase calls, are widened to 16 here).
   const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
   rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
   if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
   if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, t->side[1]);
-  // Join even after an error, so that the side streams never run ahead of
-  // the caller's stream.
-  for (int k = 0; k < 2; ++k) {
-    if (cudaEventRecord(t->ev_join[k], t->side[k]) != cudaSuccess ||
-        cudaStreamWaitEvent(s, t->ev_join[k], 0) != cudaSuccess)
-      rc = rc ? rc : MT_ERR_CUDA;
-  }
-  return rc;
+  return host_join(t, s, rc);
 }
 
 template <int T, bool CONC>
@@ -532,14 +554,13 @@ int mt_erase(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t
 int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, uint32_t maxK,
                    const uint32_t* klens, uint32_t* values, uint32_t maxV, uint32_t* vlens, bool* results,
                    uint32_t n, uint32_t flags, void* stream) {
-  (void)flags;
   if (!t || (n && (!types || !keys || !values || !vlens || maxK == 0 || maxV == 0))) return MT_ERR_INVALID_ARG;
   batch_args a{};
   a.types = types; a.keys = keys; a.key_lengths = klens; a.values = values;
   a.value_lengths_in = vlens; a.value_lengths_out = vlens; a.results = results;
   a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
   if (flags & MT_FLAG_SINGLE_PASS) return launch_batch<OP_MIXED, true>(t, a, (cudaStream_t)stream);
-  return launch_mixed_split(t, a, (cudaStream_t)stream);
+  return launch_mixed_split(t, a, (flags & MT_FLAG_BUCKET_KEYS) != 0, (cudaStream_t)stream);
 }
 
 int mt_scan(mt_masstree* t, const uint32_t* lower, const uint32_t* lower_lens, uint32_t maxK, uint32_t max_count,

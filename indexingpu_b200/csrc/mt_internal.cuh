@@ -190,6 +190,8 @@ namespace mtb {
 // Host helpers implemented in mt_capi.cu.
 int host_max_blocks_per_sm(const void* fn, int block, size_t smem);
 int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
+int host_fork(mt_masstree* t, cudaStream_t s);
+int host_join(mt_masstree* t, cudaStream_t s, int rc);
 bool host_valid_tile(uint32_t ts);
 }  // namespace mtb
 

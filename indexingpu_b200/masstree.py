@@ -27,6 +27,7 @@ from . import _lib
 
 REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
 FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS, FLAG_BUCKET_KEYS = 1, 2, 4, 8, 16
+FLAG_PERSISTENT = 32
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
@@ -140,10 +141,11 @@ class GpuMasstree:
         self._check(rc, "mt_scan")
 
     def mixed_batch(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
-                    value_lengths, results, num_requests, stream=0, single_pass=False):
+                    value_lengths, results, num_requests, stream=0, single_pass=False, bucket_keys=False):
+        flags = (FLAG_SINGLE_PASS if single_pass else 0) | (FLAG_BUCKET_KEYS if bucket_keys else 0)
         rc = self._lib.mt_mixed_batch(self._h, _ptr(request_types), _ptr(keys), max_key_length, _ptr(key_lengths),
                                       _ptr(values), max_value_length, _ptr(value_lengths), _ptr(results),
-                                      num_requests, FLAG_SINGLE_PASS if single_pass else 0, _stream(stream))
+                                      num_requests, flags, _stream(stream))
         self._check(rc, "mt_mixed_batch")
 
     # -- many sub-batches in one persistent launch --------------------------------
@@ -151,12 +153,14 @@ class GpuMasstree:
         self._check(self._lib.mt_batches_reserve(self._h, max_subbatches, max_total_requests), "mt_batches_reserve")
 
     def mixed_batches(self, descriptors, num_subbatches, max_key_length, max_value_length, stream=0,
-                      bucket_keys=False):
-        """Serve num_subbatches mixed batches in order in one persistent launch.
-        `descriptors` is a device tensor holding mt_subbatch records (see
-        pack_subbatches)."""
+                      bucket_keys=False, persistent=False):
+        """Serve num_subbatches mixed batches in order (three class kernels per
+        sub-batch on forked streams, or one persistent launch for all with
+        persistent=True).  `descriptors` is a device tensor holding
+        mt_subbatch records (see pack_subbatches)."""
+        flags = (FLAG_BUCKET_KEYS if bucket_keys else 0) | (FLAG_PERSISTENT if persistent else 0)
         rc = self._lib.mt_mixed_batches(self._h, _ptr(descriptors), num_subbatches, max_key_length,
-                                        max_value_length, FLAG_BUCKET_KEYS if bucket_keys else 0, _stream(stream))
+                                        max_value_length, flags, _stream(stream))
         self._check(rc, "mt_mixed_batches")
 
     # -- serving ---------------------------------------------------------------------

@@ -147,7 +147,7 @@ class GpuIndex(_TorchIndex):
         self.t.sync()
         return self.h(vals), self.h(vlens)
 
-    def mixed(self, types, keys, klens, vals, vlens, n=None):
+    def mixed(self, types, keys, klens, vals, vlens, n=None, bucket_keys=False):
         torch = self.torch
         keys = _u32(keys)
         n = len(keys) if n is None else n
@@ -155,7 +155,7 @@ class GpuIndex(_TorchIndex):
         dvl = self.d(_u32(vlens))
         res = self.zeros(n, torch.bool)
         self.t.mixed_batch(self.d(np.ascontiguousarray(types, np.uint8)), self.d(keys), keys.shape[1],
-                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n)
+                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n, bucket_keys=bucket_keys)
         self.t.sync()
         return self.h(dv), self.h(dvl), self.h(res).astype(np.uint8)
 

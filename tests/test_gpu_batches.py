@@ -70,9 +70,10 @@ def _check_outputs(ref_sb, new_sb, bt):
         assert np.array_equal(gv[i, :c], ev[i, :c]), i
 
 
+@pytest.mark.parametrize("persistent", [False, True])
 @pytest.mark.parametrize("tf,tw,bucket", [(8, 32, False), (8, 32, True), (4, 16, True), (16, 32, False),
                                           (32, 32, True)])
-def test_mixed_batches_match_per_call(tf, tw, bucket):
+def test_mixed_batches_match_per_call(tf, tw, bucket, persistent):
     import torch
     c2 = wl.C2(n_preload=20000, n_prefixes=64)
     ref, new = _make_pair(torch, c2, 20000, tf, tw)
@@ -87,7 +88,7 @@ def test_mixed_batches_match_per_call(tf, tw, bucket):
         ref.sync()
         desc = torch.from_numpy(pack_subbatches(new_sbs)).cuda()
         new.reserve_batches(len(new_sbs), sum(sb["n"] for sb in new_sbs))
-        new.mixed_batches(desc, len(new_sbs), MAXK, MAXV, bucket_keys=bucket)
+        new.mixed_batches(desc, len(new_sbs), MAXK, MAXV, bucket_keys=bucket, persistent=persistent)
         new.sync()
         for r, s, bt in zip(ref_sbs, new_sbs, bts):
             _check_outputs(r, s, bt)
@@ -99,7 +100,8 @@ def test_mixed_batches_match_per_call(tf, tw, bucket):
         new.close()
 
 
-def test_mixed_batches_graph_replay():
+@pytest.mark.parametrize("persistent", [False, True])
+def test_mixed_batches_graph_replay(persistent):
     """Capture one mt_mixed_batches call in a CUDA graph, then replay it after
     rewriting the sub-batch buffers in place with the next batches' data."""
     import torch
@@ -145,11 +147,11 @@ def test_mixed_batches_graph_replay():
         load(plans[0])
         s = torch.cuda.Stream()
         with torch.cuda.stream(s):
-            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s)
+            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent)
         new.sync(s)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=s):
-            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s)
+            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent)
         for r in range(1, rounds):
             load(plans[r])
             g.replay()
@@ -195,7 +197,7 @@ def test_autotune_small_cases():
                         max_key_length=MAXK, max_value_length=MAXV, keep=(d, res))
 
         best, trials = autotune.tune(t, make_case, blocks_per_sm=(2, 8))
-        assert len(trials) == 16 + 2
+        assert len(trials) == 32 + 2
         assert best["find_tile"] in autotune.FIND_TILES and best["write_tile"] in autotune.WRITE_TILES
         assert all(tr["mops"] > 0 for tr in trials)
         ok, _, report = t.validate()

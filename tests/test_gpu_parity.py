@@ -105,8 +105,9 @@ def _touch_once_batches(c2, n_batches, n):
     return out
 
 
+@pytest.mark.parametrize("bucket", [False, True])
 @pytest.mark.parametrize("n_preload", [3000, 40000])
-def test_c2_mixed_touch_once(tile, n_preload):
+def test_c2_mixed_touch_once(tile, n_preload, bucket):
     c2 = wl.C2(n_preload=n_preload, n_prefixes=64)
     keys, lens, vals, vlens = c2.keys(np.arange(n_preload))
     g, o = GpuIndex(tile), OracleIndex()
@@ -114,7 +115,7 @@ def test_c2_mixed_touch_once(tile, n_preload):
         g.insert(keys, lens, vals, vlens)
         o.insert(keys, lens, vals, vlens)
         for bt in _touch_once_batches(c2, 4, 8000):
-            gv, gl, gr = g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
+            gv, gl, gr = g.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"], bucket_keys=bucket)
             ov, ol, orr = o.mixed(bt["types"], bt["keys"], bt["lens"], bt["vals"], bt["vlens"])
             notfind = bt["types"] != wl.REQ_FIND
             np.testing.assert_array_equal(gr[notfind], orr[notfind], err_msg="mixed results")

@@ -11,6 +11,7 @@ def test_autotune_coordinate_descent_picks_the_best():
     # on, 6 blocks per SM.
     def score(c):
         s = 100.0 - abs(c["find_tile"] - 8) - (0 if c["write_tile"] == 32 else 7) + (3 if c["bucketing"] else 0)
+        s -= 0 if c["form"] == "forked" else 5
         b = c["blocks_per_sm"] or 8
         return s - abs(b - 6)
 
@@ -28,10 +29,11 @@ def test_autotune_coordinate_descent_picks_the_best():
 
     best, trials = autotune.tune(None, make_case, trial=trial)
     assert (best["find_tile"], best["write_tile"], best["bucketing"], best["blocks_per_sm"]) == (8, 32, True, 6)
-    assert len(trials) == 4 * 2 * 2 + 8
-    # One warm-up case for all eight kernel flavours, then a fresh case per trial.
+    assert best["form"] == "forked"
+    assert len(trials) == 2 * 4 * 2 * 2 + 8
+    # One warm-up case for all sixteen kernel flavours, then a fresh case per trial.
     assert cases == list(range(len(trials) + 1))
-    assert sum(1 for i, _ in seen if i == 0) == 8
+    assert sum(1 for i, _ in seen if i == 0) == 16
     assert best["mops"] == max(t["mops"] for t in trials)
 
 
