@@ -53,20 +53,17 @@ constexpr uint32_t META_VERSION_ONE = 1u << 16;
 
 constexpr int WORD_CSUM = 26, WORD_HIGH = 28, WORD_SIB = 29, WORD_META = 30, WORD_KS = 31;
 
-// lowbias32 integer hash (C. Wellons, "Prospecting for Hash Functions", 2018).
-MT_HD uint32_t mix32(uint32_t x) {
-  x ^= x >> 16;
-  x *= 0x7FEB352Du;
-  x ^= x >> 15;
-  x *= 0x846CA68Bu;
-  x ^= x >> 16;
-  return x;
-}
-// Contribution of word g (value v) to a node checksum.
+// Contribution of word g (value v) to a node checksum: a bijection of v for
+// every position (xor with a position constant, multiply by an odd constant,
+// xor-shift), so a torn image differing from a published one in a single word
+// always fails, and one differing in several words passes only if their mixed
+// differences cancel exactly modulo 2^32.  (One multiply per word: the
+// verification runs on every lock-free node load.)
 MT_HD uint32_t csum_term(uint32_t g, uint32_t v) {
   if (g == (uint32_t)WORD_CSUM) return 0u;
   if (g == (uint32_t)WORD_META) v &= ~(1u << 4);  // LOCK bit changes without a republish
-  return mix32(v ^ (g * 0x9E3779B9u) ^ 0x5BD1E995u);
+  const uint32_t x = (v ^ (g * 0x9E3779B9u) ^ 0x5BD1E995u) * 0x7FEB352Du;
+  return x ^ (x >> 15);
 }
 // Host/device checksum of a full 32-word node image.
 MT_HD uint32_t node_checksum(const uint32_t* w) {

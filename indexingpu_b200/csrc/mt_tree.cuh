@@ -62,10 +62,11 @@ MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
   t.sync();
 }
 
-// Test-and-test-and-set: waiters poll the meta word with plain loads and only
-// try the atomic when it reads unlocked, with jittered exponential backoff
-// (64 ns .. 4 us), so a hot node's holder is not slowed by a storm of atomics
-// on its line.
+// The first attempt goes straight to the atomic (an uncontended lock costs one
+// round trip); after a failure it is test-and-test-and-set: waiters poll the
+// meta word with plain loads and only try the atomic when it reads unlocked,
+// with jittered exponential backoff (64 ns .. 4 us), so a hot node's holder is
+// not slowed by a storm of atomics on its line.
 template <int T>
 MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T>& nd) {
   uint32_t* mw = p.addr(idx) + WORD_META;
@@ -74,7 +75,7 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
   for (uint32_t it = 0; it < kLockSpins; ++it) {
     uint32_t old = META_LOCK;
     if (t.leader()) {
-      if (!(ld_relaxed_u32(mw) & META_LOCK)) old = atom_or_acquire(mw, META_LOCK);
+      if (it == 0u || !(ld_relaxed_u32(mw) & META_LOCK)) old = atom_or_acquire(mw, META_LOCK);
     }
     old = t.shfl(old, 0);
     if (!(old & META_LOCK)) {
