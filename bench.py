@@ -7,9 +7,10 @@ preload; keys 2-16 slices sharing 4096 four-slice prefixes, values 1-8 slices).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl ours (default) prints one JSON line with the device-resident throughput
-(`value`), the end-to-end throughput through the C ABI with host buffers copied
-in and results copied out every step (`e2e`), the roofline of the batch kernel,
-the CPU baseline and the SM clocks seen during the timed region.
+(`value`), the end-to-end throughput through the C ABI with pinned host buffers
+(`e2e`: mt_mixed_batch_host uploads every step's requests and downloads its
+results, overlapped with the work), the roofline of the batch kernel, the CPU
+baseline and the SM clocks seen during the timed region.
 --impl reference times the CPU restatement of the path (the reference's own CPU
 counterpart, masstree-beta, is not available) with every host thread, on the
 same workload.  Under torchrun each rank runs an independent replica (the index
@@ -271,29 +272,19 @@ def run_ours(args, rank, world, dist):
         abytes += alg_bytes(bt, b["vlens"].cpu().numpy(), b["res"].cpu().numpy())
     del dev_b
 
-    # End to end: pinned host buffers in, results out, every step.
+    # End to end: pinned host buffers in, results out, every step, through
+    # mt_mixed_batch_host (uploads, work and downloads of consecutive chunks
+    # overlap, also across steps).
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
     host = [dict(types=pin(bt["types"]), keys=pin(bt["keys"]), lens=pin(bt["lens"]), vals=pin(bt["vals"]),
-                 vlens=pin(bt["vlens"])) for bt in e2e_batches]
-    out = dict(vals=torch.empty((args.batch, MAXV), dtype=torch.uint32).pin_memory(),
-               vlens=torch.empty(args.batch, dtype=torch.uint32).pin_memory(),
-               res=torch.empty(args.batch, dtype=torch.bool).pin_memory())
-    dbuf = dict(types=torch.empty(args.batch, dtype=torch.uint8, device="cuda"),
-                keys=torch.empty((args.batch, MAXK), dtype=torch.uint32, device="cuda"),
-                lens=torch.empty(args.batch, dtype=torch.uint32, device="cuda"),
-                vals=torch.empty((args.batch, MAXV), dtype=torch.uint32, device="cuda"),
-                vlens=torch.empty(args.batch, dtype=torch.uint32, device="cuda"),
-                res=torch.empty(args.batch, dtype=torch.bool, device="cuda"))
-    h2d = sum(host[0][k].numel() * host[0][k].element_size() for k in host[0])
-    d2h = sum(out[k].numel() * out[k].element_size() for k in out)
+                 vlens=pin(bt["vlens"]), res=torch.zeros(args.batch, dtype=torch.bool).pin_memory())
+            for bt in e2e_batches]
+    h2d = sum(host[0][k].numel() * host[0][k].element_size() for k in ("types", "keys", "lens", "vals", "vlens"))
+    d2h = sum(host[0][k].numel() * host[0][k].element_size() for k in ("vals", "vlens", "res"))
 
     def e2e_step(h):
-        for k in ("types", "keys", "lens", "vals", "vlens"):
-            dbuf[k].copy_(h[k], non_blocking=True)
-        tree.mixed_batch(dbuf["types"], dbuf["keys"], MAXK, dbuf["lens"], dbuf["vals"], MAXV, dbuf["vlens"],
-                         dbuf["res"], args.batch, stream=stream, bucket_keys=bool(args.bucket))
-        for k in ("vals", "vlens", "res"):
-            out[k].copy_(dbuf[k], non_blocking=True)
+        tree.mixed_batch_host(h["types"], h["keys"], MAXK, h["lens"], h["vals"], MAXV, h["vlens"], h["res"],
+                              args.batch, stream=stream, bucket_keys=bool(args.bucket))
 
     for i in range(e2e_w):
         e2e_step(host[i])
@@ -313,7 +304,7 @@ def run_ours(args, rank, world, dist):
     extra = {}
     wanted = set() if args.sections == "none" else set(args.sections.split(","))
     if world == 1:
-        del host, out, dbuf
+        del host
         if "batched" in wanted:
             extra["batched"] = run_batched(args, tree, c2, stream)
         if "served" in wanted:
@@ -360,7 +351,9 @@ def run_ours(args, rank, world, dist):
                                  "p99": round(sorted_steps[min(len(sorted_steps) - 1,
                                                                int(0.99 * len(sorted_steps)))], 4)},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_k},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_k,
+                    "call": "mt_mixed_batch_host (pinned host buffers; chunked uploads, work and downloads "
+                            "overlapped)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": None if tr is None else int(tr * args.batch),

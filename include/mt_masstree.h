@@ -136,6 +136,25 @@ int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32
                    uint32_t max_value_length, uint32_t* value_lengths, bool* results,
                    uint32_t num_requests, uint32_t flags, void* stream);
 
+/* mt_mixed_batch with every buffer in HOST memory (pinned for the copies to
+ * overlap): the batch is cut into chunks of `chunk` requests (0 = 262,144)
+ * that go through a ring of device staging slots kept by the tree; the
+ * uploads, the work and the downloads of consecutive chunks overlap, also
+ * across consecutive calls on one tree.  Each chunk is served as one
+ * mt_mixed_batch (one of the orders a mixed batch allows).  Asynchronous:
+ * the input buffers are read from the moment of the call on (they must hold
+ * the requests then, and the uploads do not wait for earlier work on
+ * `stream`), the work and the results are ordered on `stream`, and all host
+ * buffers must stay untouched until the stream reaches the end of the call
+ * (results are in host memory then).  The first call, and a
+ * call with longer rows or larger chunks than before, allocates the staging
+ * (not during graph capture).  New in this library: the reference's caller
+ * copies around each device-buffer call itself. */
+int mt_mixed_batch_host(mt_masstree* tree, const uint8_t* request_types, const uint32_t* keys,
+                        uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
+                        uint32_t max_value_length, uint32_t* value_lengths, bool* results,
+                        uint32_t num_requests, uint32_t chunk, uint32_t flags, void* stream);
+
 /* Size the scratch of mt_mixed_batches for up to max_subbatches sub-batches
  * and max_total_requests requests in one call (allocates; call it before any
  * graph capture).  New in this library. */

@@ -25,6 +25,7 @@ SIGNATURES = {
     "mt_scan": (_int, [_p, _p, _p, _u32, _u32, _u32, _p, _p, _p, _p, _u32, _p, _p, _p, _u32, _p]),
     "mt_mixed_batch": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _u32, _p]),
     "mt_mixed_batch_noalloc": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _p]),
+    "mt_mixed_batch_host": (_int, [_p, _p, _p, _u32, _p, _p, _u32, _p, _p, _u32, _u32, _u32, _p]),
     "mt_batches_reserve": (_int, [_p, _u32, _u64]),
     "mt_mixed_batches": (_int, [_p, _p, _u32, _u32, _u32, _u32, _p]),
     "mt_sync": (_int, [_p, _p]),

@@ -481,6 +481,7 @@ int mt_destroy(mt_masstree* t) {
   if (t->frames) cudaFree(t->frames);
   if (t->split_idx) cudaFree(t->split_idx);
   if (t->batches_mem) cudaFree(t->batches_mem);
+  host_pipe_free(t);
   if (t->mem) cudaFree(t->mem);
   if (t->h_err) cudaFreeHost(t->h_err);
   for (int k = 0; k < 2; ++k) {

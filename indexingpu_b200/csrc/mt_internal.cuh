@@ -161,6 +161,8 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
 
 }  // namespace mtb
 
+struct mt_host_pipe;  // staging of mt_mixed_batch_host (mt_host.cu)
+
 struct mt_masstree {
   // Host-side state of one tree.
   int device = 0;
@@ -175,6 +177,7 @@ struct mt_masstree {
   cudaStream_t side[2] = {nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[2] = {nullptr, nullptr};
+  mt_host_pipe* host_pipe = nullptr;
   void* mem = nullptr;
   mtb::tree_view tv{};
   mtb::scan_frame* frames = nullptr;
@@ -192,6 +195,7 @@ int host_max_blocks_per_sm(const void* fn, int block, size_t smem);
 int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
 int host_fork(mt_masstree* t, cudaStream_t s);
 int host_join(mt_masstree* t, cudaStream_t s, int rc);
+void host_pipe_free(mt_masstree* t);  // mt_host.cu
 bool host_valid_tile(uint32_t ts);
 }  // namespace mtb
 

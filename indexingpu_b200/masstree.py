@@ -148,7 +148,18 @@ class GpuMasstree:
                                       num_requests, flags, _stream(stream))
         self._check(rc, "mt_mixed_batch")
 
-    # -- many sub-batches in one persistent launch --------------------------------
+    def mixed_batch_host(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
+                         value_lengths, results, num_requests, stream=0, chunk=0, bucket_keys=False):
+        """mixed_batch with every buffer in (pinned) host memory; uploads, work and
+        downloads of consecutive chunks overlap.  Asynchronous: sync(stream)
+        before reading the results or reusing the buffers."""
+        rc = self._lib.mt_mixed_batch_host(self._h, _ptr(request_types), _ptr(keys), max_key_length,
+                                           _ptr(key_lengths), _ptr(values), max_value_length, _ptr(value_lengths),
+                                           _ptr(results), num_requests, chunk,
+                                           FLAG_BUCKET_KEYS if bucket_keys else 0, _stream(stream))
+        self._check(rc, "mt_mixed_batch_host")
+
+    # -- many sub-batches in one call ------------------------------------------------
     def reserve_batches(self, max_subbatches, max_total_requests):
         self._check(self._lib.mt_batches_reserve(self._h, max_subbatches, max_total_requests), "mt_batches_reserve")
 
