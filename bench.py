@@ -55,10 +55,11 @@ def parse():
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
     ap.add_argument("--pool-gb", type=float, default=0.0,
                     help="slab pool size in GB (default: 60%% of the free device memory)")
-    ap.add_argument("--sections", default="batched,served",
+    ap.add_argument("--sections", default="batched,served,c1,c3",
                     help="extra measurements at N=1: batched (256 sub-batches, tuned persistent launch from a "
                          "CUDA graph, against one call per sub-batch), served (request loop over 64M keys, "
-                         "latency against offered load, against one call per request); 'none' to skip")
+                         "latency against offered load, against one call per request), c1 (plain insert and "
+                         "find, 1M keys), c3 (range scan, 32M keys); 'none' to skip")
     ap.add_argument("--subbatches", type=int, default=256)
     ap.add_argument("--tune-subbatches", type=int, default=16, help="sub-batches per autotuner trial")
     ap.add_argument("--serve-keys", type=int, default=1 << 26, help="tree size for the served section")
@@ -310,6 +311,13 @@ def run_ours(args, rank, world, dist):
         if "served" in wanted:
             extra["served"] = run_served(args, tree, c2, stream)
     tree.close()
+    if world == 1 and ("c1" in wanted or "c3" in wanted):
+        del tree
+        peak_c, _ = measured_peak()
+        if "c1" in wanted:
+            extra["c1"] = run_c1(args, stream, peak_c)
+        if "c3" in wanted:
+            extra["c3"] = run_c3(args, stream, peak_c)
 
     # Reduce over ranks: max time.
     if dist:
@@ -513,6 +521,105 @@ def run_served(args, tree, c2, stream):
             "plain_per_request_peak": plain_peak, "plain_at_half_its_peak": plain_half,
             "served_at_same_load": served_half,
             "served_over_plain_mops": round(peak["mops"] / plain_peak["mops"], 2)}
+
+
+def _timed(stream, fn, reps=1):
+    """Device time of reps calls of fn on stream (ms per call)."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_c1(args, stream, peak):
+    """1M distinct keys of 1-8 random slices, 2-slice values: bulk insert, then
+    1M finds (half hits, half absent keys), each timed on the device."""
+    import torch
+    from indexingpu_b200 import GpuMasstree
+    d = wl.c1()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    k, l, v, vl = dev(d["keys"]), dev(d["lens"]), dev(d["vals"]), dev(d["vlens"])
+    fk, fl = dev(d["find_keys"]), dev(d["find_lens"])
+    n, nf, mk, mv = len(d["keys"]), len(d["find_keys"]), d["maxK"], d["maxV"]
+    out_v = torch.zeros((nf, mv), dtype=torch.uint32, device="cuda")
+    out_l = torch.zeros(nf, dtype=torch.uint32, device="cuda")
+    with GpuMasstree(pool_bytes=2 << 30, tile_size=args.tile) as t:
+        t.set_write_tile_size(args.write_tile)
+        ins_ms = _timed(stream, lambda: t.insert(k, mk, l, v, mv, vl, n, stream=stream))
+        t.sync(stream)
+        find = lambda: t.find(fk, mk, fl, out_v, mv, out_l, nf, stream=stream)  # noqa: E731
+        for _ in range(3):
+            find()
+        find_ms = _timed(stream, find, reps=10)
+        t.sync(stream)
+    got = out_l.cpu().numpy()
+    hits = int((got > 0).sum())
+    assert hits == int(d["find_hit"].sum()), "C1 find hits differ from the generator's"
+    # Compulsory bytes per find: request I/O + border line + value chain line on
+    # a hit (2-slice values of 1-slice keys and the key rests of longer keys
+    # live in chains).
+    L = d["find_lens"].astype(np.int64)
+    fb = int((4 * L + 4 + np.where(d["find_hit"], 4 * mv + 4 + 256, 4 + 128)).sum())
+    ach = fb / (find_ms / 1e3) / 1e9
+    return {"workload": "1M distinct keys of 1-8 random slices, 2-slice values; 1M finds, 50% hits",
+            "insert_mops": round(n / ins_ms / 1e3, 2), "find_mops": round(nf / find_ms / 1e3, 2),
+            "find_hits": hits,
+            "find_roofline": {"achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
+                              "frac": round(ach / peak, 4), "algorithmic_bytes": fb,
+                              "note": "the 1M-key index (~150 MB of slabs) is mostly L2-resident"}}
+
+
+def run_c3(args, stream, peak):
+    """32M fixed 2-slice keys (big-endian halves of random u64s), 1-slice
+    values; 1M scans from random lower bounds, up to 100 results each, keys,
+    values and lengths returned."""
+    import torch
+    from indexingpu_b200 import GpuMasstree
+    n, nq, mc = 1 << 25, 1 << 20, 100
+    d = wl.c3(n, nq)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    lo, lol = dev(d["lower"]), dev(d["lower_lens"])
+    counts = torch.zeros(nq, dtype=torch.uint32, device="cuda")
+    vals = torch.zeros((nq, mc, 1), dtype=torch.uint32, device="cuda")
+    vlens = torch.zeros((nq, mc), dtype=torch.uint32, device="cuda")
+    okeys = torch.zeros((nq, mc, 2), dtype=torch.uint32, device="cuda")
+    oklens = torch.zeros((nq, mc), dtype=torch.uint32, device="cuda")
+    with GpuMasstree(pool_bytes=8 << 30, tile_size=args.tile) as t:
+        t.set_write_tile_size(args.write_tile)
+        step = 1 << 20
+        for s0 in range(0, n, step):
+            sl = slice(s0, s0 + step)
+            t.insert(dev(d["keys"][sl]), 2, dev(d["lens"][sl]), dev(d["vals"][sl]), 1, dev(d["vlens"][sl]),
+                     min(step, n - s0), stream=stream)
+        t.sync(stream)
+        scan = lambda: t.scan(lo, lol, 2, mc, nq, counts=counts, values=vals, max_value_length=1,  # noqa: E731
+                              value_lengths=vlens, out_keys=okeys, out_key_lengths=oklens, stream=stream)
+        scan()
+        scan_ms = _timed(stream, scan, reps=3)
+        t.sync(stream)
+    c = counts.cpu().numpy().astype(np.int64)
+    results = int(c.sum())
+    # Sortedness of every query's output keys (as u64), checked on a sample.
+    ok = okeys[:1024].cpu().numpy().astype(np.uint64)
+    kk = (ok[:, :, 0] << np.uint64(32)) | ok[:, :, 1]
+    for q in range(1024):
+        assert np.all(kk[q, 1:c[q]] > kk[q, :c[q] - 1]), q
+    # Compulsory bytes per query: lower key, the border lines the results span
+    # (13 entries per node at most), one suffix line per result (key rest and
+    # value), and the output rows.
+    fb = int((8 + 128 * (np.ceil(c / 13.0) + 1) + 128 * c + c * (8 + 4 + 4 + 4) + 4).sum())
+    ach = fb / (scan_ms / 1e3) / 1e9
+    return {"workload": "32M keys of 2 slices, 1-slice values; 1M scans of up to 100 results from random lower "
+                        "bounds (keys, values, lengths returned)",
+            "scan_queries_per_s_M": round(nq / scan_ms / 1e3, 3), "results_per_s_M": round(results / scan_ms / 1e3, 2),
+            "mean_results": round(results / nq, 2),
+            "scan_roofline": {"achieved": round(ach, 2), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+                              "algorithmic_bytes": fb}}
 
 
 def run_reference(args, rank):
