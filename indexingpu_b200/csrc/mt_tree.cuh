@@ -31,7 +31,7 @@
 namespace mtb {
 
 constexpr uint32_t kMaxHops = 1u << 16;     // node visits per operation
-constexpr uint32_t kLockSpins = 1u << 18;   // lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
+constexpr uint32_t kLockSpins = 1u << 20;   // lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
 constexpr uint32_t kMaxRestarts = 1u << 14;
 
 #ifndef MT_CONC_LOAD
@@ -65,7 +65,7 @@ MT_DEV void unlock_node(const tile<T>& t, const pool_view& p, uint32_t idx) {
 // The first attempt goes straight to the atomic (an uncontended lock costs one
 // round trip); after a failure it is test-and-test-and-set: waiters poll the
 // meta word with plain loads and only try the atomic when it reads unlocked,
-// with jittered exponential backoff (64 ns .. 4 us), so a hot node's holder is
+// with jittered exponential backoff (64 ns .. 1 us), so a hot node's holder is
 // not slowed by a storm of atomics on its line.
 template <int T>
 MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T>& nd) {
@@ -87,7 +87,7 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
     jitter = jitter * 1664525u + 1013904223u;
     __nanosleep(backoff + ((jitter >> 16) & (backoff - 1u)));
-    if (backoff < 2048u) backoff <<= 1;
+    if (backoff < 512u) backoff <<= 1;
   }
   if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT);
   return false;
