@@ -199,6 +199,20 @@ def cpu_run(preload_data, batches, threads):
 
 # ---- GPU leg -------------------------------------------------------------------------
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of per-rank times over all ranks (every rank gets it)."""
+    import torch
+    t = torch.tensor(values, device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(requests_per_rank, world, ms):
+    """Mops/s of the whole job: every rank's requests over the slowest rank's time
+    (replicas: each rank serves its own index, weak scaling)."""
+    return requests_per_rank * world / (ms / 1e3) / 1e6
+
+
 def run_ours(args, rank, world, dist):
     import torch
     from indexingpu_b200 import GpuMasstree
@@ -321,12 +335,9 @@ def run_ours(args, rank, world, dist):
 
     # Reduce over ranks: max time.
     if dist:
-        t = torch.tensor([total_ms, e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0]), float(t[1])
-    reqs = args.steps * args.batch * world
-    value = reqs / (total_ms / 1e3) / 1e6
-    e2e_value = e2e_k * args.batch * world / (e2e_ms / 1e3) / 1e6
+        total_ms, e2e_ms = max_over_ranks(dist, [total_ms, e2e_ms], "cuda")
+    value = whole_job_rate(args.steps * args.batch, world, total_ms)
+    e2e_value = whole_job_rate(e2e_k * args.batch, world, e2e_ms)
 
     res = None
     if rank == 0:
