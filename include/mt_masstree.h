@@ -192,7 +192,8 @@ typedef struct mt_serve_plan {
   bool* results;               /* may be NULL */
   uint32_t max_key_length;
   uint32_t max_value_length;
-  /* Host arrays, one entry per request, in arrival order. */
+  /* Host arrays, one entry per request, in arrival order; the op ranges of
+   * different requests must not overlap. */
   const uint32_t* request_first_op;
   const uint32_t* request_num_ops;
   const uint64_t* arrival_ns;  /* arrival time after the start of the run */

@@ -70,6 +70,7 @@ struct server_view {
   uint32_t* finished;                   // device: finished items per request
   uint32_t* done;                       // mapped host: per-request completion flags
   uint32_t ring_cap;
+  const uint32_t* order;                // device: op indexes, every request's ops grouped by kind
   batch_args ops;                       // op arrays of all requests
 };
 
@@ -175,18 +176,14 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) server_kernel(tr
     leave = __shfl_sync(0xFFFFFFFFu, leave, 0);
     if (leave) break;
     const serve_item it = ld_item(sv.ring + (c % sv.ring_cap));
+    // The item's ops, through the kind-grouped order: the tiles of a warp
+    // mostly serve ops of one kind side by side (one code path, no
+    // divergence between find and write paths).
     batch_args a = sv.ops;
-    a.index = nullptr;
+    a.index = sv.order + it.first;
     a.n_dev = nullptr;
     a.n_back_dev = nullptr;
     a.n = it.count;
-    a.types += it.first;
-    a.keys += (size_t)it.first * a.max_key_length;
-    if (a.key_lengths) a.key_lengths += it.first;
-    a.values += (size_t)it.first * a.max_value_length;
-    a.value_lengths_in += it.first;
-    a.value_lengths_out += it.first;
-    if (a.results) a.results += it.first;
     serve_requests<T, OP_MIXED, true>(t, tv, cache, a, tile_in_warp, tiles_per_warp);
     __syncwarp();
     if (lane == 0) {
@@ -291,6 +288,15 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     total_ops = std::max<uint64_t>(total_ops, (uint64_t)plan->request_first_op[r] + plan->request_num_ops[r]);
   }
   if (total_ops > 0xFFFFFFFFull) return MT_ERR_INVALID_ARG;
+  {
+    // Every op belongs to at most one request.
+    std::vector<uint8_t> owned(std::max<uint64_t>(total_ops, 1), 0);
+    for (uint32_t r = 0; r < nreq; ++r)
+      for (uint32_t o = plan->request_first_op[r]; o < plan->request_first_op[r] + plan->request_num_ops[r]; ++o) {
+        if (owned[o]) return MT_ERR_INVALID_ARG;
+        owned[o] = 1;
+      }
+  }
   // Work-item size: fixed, or (chunk_ops == 0) chosen per request from the
   // backlog, from one op per tile of a warp while the device has idle tiles
   // (lowest latency) up to eight per tile under load (fewer items per op).
@@ -368,6 +374,7 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     uint32_t *d_stop = nullptr, *d_done = nullptr, *d_finished = nullptr;
     unsigned long long* d_usage = nullptr;
     unsigned long long* d_held = nullptr;
+    uint32_t* d_order = nullptr;
     server_ctl* d_ctl = nullptr;
     const int blocks = server_blocks_tile(t);
     const size_t nwarps = (size_t)blocks * (kBlock / 32);
@@ -383,6 +390,25 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
                  cudaMemset(d_held, 0xFF, nwarps * sizeof(unsigned long long)) == cudaSuccess &&
                  cudaMemset(d_finished, 0, (size_t)nreq * sizeof(uint32_t)) == cudaSuccess &&
                  cudaMemset(d_ctl, 0, sizeof(server_ctl)) == cudaSuccess;
+    if (ok) {
+      // Every request's ops in the order finds, inserts, updates and erases
+      // (a request's ops have no order among each other, as in one mixed
+      // batch), so that items cut from it are mostly of one kind.
+      std::vector<uint32_t> order(std::max<uint64_t>(total_ops, 1));
+      for (uint32_t r = 0; r < nreq; ++r) {
+        const uint32_t f = plan->request_first_op[r], no = plan->request_num_ops[r];
+        uint32_t pos = f;
+        for (uint8_t kind : {(uint8_t)MT_REQ_FIND, (uint8_t)MT_REQ_INSERT, (uint8_t)MT_REQ_UPDATE,
+                             (uint8_t)MT_REQ_ERASE})
+          for (uint32_t o = f; o < f + no; ++o)
+            if (h_types[o] == kind) order[pos++] = o;
+        for (uint32_t o = f; o < f + no; ++o)  // unknown kinds: served (and reported) last
+          if (h_types[o] > MT_REQ_UPDATE) order[pos++] = o;
+      }
+      ok = cudaMalloc(&d_order, order.size() * sizeof(uint32_t)) == cudaSuccess &&
+           cudaMemcpy(d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) ==
+               cudaSuccess;
+    }
     if (usage) *usage = (unsigned long long)slabs_in_use;
     server_view sv{};
     sv.ring = d_ring;
@@ -393,6 +419,7 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     sv.finished = d_finished;
     sv.done = d_done;
     sv.ring_cap = (uint32_t)std::min<uint64_t>(total_items, 0xFFFFFFFFull);
+    sv.order = d_order;
     sv.ops = ops;
     const unsigned long long epoch_ns = (unsigned long long)(plan->epoch_us ? plan->epoch_us : 20000u) * 1000ull;
     if (ok) {
@@ -529,6 +556,7 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     if (d_finished) cudaFree(d_finished);
     if (d_ctl) cudaFree(d_ctl);
     if (d_held) cudaFree(d_held);
+    if (d_order) cudaFree(d_order);
   }
   cudaStreamSynchronize(s);
   cudaStreamDestroy(s);

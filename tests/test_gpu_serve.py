@@ -144,6 +144,11 @@ def test_serve_rejects_bad_plans():
         bad["arrival_ns"] = st["arrival_ns"][::-1].copy()  # not in arrival order
         with pytest.raises(MasstreeError):
             _serve(torch, tree, bad)
+        overlap = dict(st)
+        overlap["first"] = st["first"].copy()
+        overlap["first"][1] = st["first"][0]  # request 1 reuses request 0's ops
+        with pytest.raises(MasstreeError):
+            _serve(torch, tree, overlap)
         # The tree is still usable.
         _serve(torch, tree, st)
     finally:
