@@ -298,12 +298,14 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
       }
   }
   // Work-item size: fixed, or (chunk_ops == 0) chosen per request from the
-  // backlog, from one op per tile of a warp while the device has idle tiles
-  // (lowest latency) up to eight per tile under load (fewer items per op).
+  // backlog (ops admitted and not complete): one op per item (a warp each,
+  // lowest latency) while the backlog is below an eighth of the grid's warps, then
+  // one, two, four or eight ops per tile of a warp as it grows (fewer items
+  // per op: one-op items cap the loop at about a sixth of its peak).
   const uint32_t tiles_per_warp = 32u / t->tile_size;
   const bool auto_chunk = plan->chunk_ops == 0;
   const uint32_t fixed_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(plan->chunk_ops, 4096u));
-  const uint32_t min_chunk = auto_chunk ? tiles_per_warp : fixed_chunk;
+  const uint32_t min_chunk = auto_chunk ? 1u : fixed_chunk;
   const double budget = plan->memory_budget > 0.f ? plan->memory_budget : 0.9;
   mt_stats_t st{};
   int rc = mt_stats(t, &st);
@@ -501,7 +503,8 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
           if (auto_chunk) {
             const uint64_t backlog = admitted_ops - std::min(admitted_ops, completed_ops.load());
             const uint64_t per_tile = backlog / total_tiles;
-            chunk = tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
+            chunk = backlog < nwarps / 8 ? 1u
+                                         : tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
           }
           const uint32_t nops = plan->request_num_ops[r];
           const uint32_t n_items = std::max<uint32_t>(1u, (nops + chunk - 1) / chunk);
