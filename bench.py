@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--write-tile", type=int, default=32, help="lanes per insert/update/erase")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--bucket", type=int, default=0, help="1: mixed_batch serves short keys before long keys")
+    ap.add_argument("--host-chunk", type=int, default=0,
+                    help="requests per chunk of mt_mixed_batch_host in the e2e leg (0: the library's default)")
     ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
@@ -299,7 +301,7 @@ def run_ours(args, rank, world, dist):
 
     def e2e_step(h):
         tree.mixed_batch_host(h["types"], h["keys"], MAXK, h["lens"], h["vals"], MAXV, h["vlens"], h["res"],
-                              args.batch, stream=stream, bucket_keys=bool(args.bucket))
+                              args.batch, stream=stream, chunk=args.host_chunk, bucket_keys=bool(args.bucket))
 
     for i in range(e2e_w):
         e2e_step(host[i])
