@@ -106,6 +106,36 @@ class gpu_masstree {
           "mt_mixed_batch");
   }
 
+  // ---- additions of this library (no counterpart in the reference) ----------
+
+  // mixed_batch with every buffer in pinned host memory; uploads, work and
+  // downloads of consecutive chunks overlap (mt_mixed_batch_host).
+  void mixed_batch_host(const request_type* request_types, const key_slice_type* keys,
+                        const size_type max_key_length, const size_type* key_lengths, value_slice_type* values,
+                        const size_type max_value_length, size_type* value_lengths, bool* results,
+                        const size_type num_requests, cudaStream_t stream = 0, const size_type chunk = 0) {
+    check(mt_mixed_batch_host(h_, reinterpret_cast<const uint8_t*>(request_types), keys, max_key_length,
+                              key_lengths, values, max_value_length, value_lengths, results, num_requests, chunk,
+                              0u, stream),
+          "mt_mixed_batch_host");
+  }
+
+  // Many mixed sub-batches in order in one call (mt_mixed_batches; device
+  // descriptors, sized beforehand by reserve_batches).
+  void reserve_batches(const size_type max_subbatches, const uint64_t max_total_requests) {
+    check(mt_batches_reserve(h_, max_subbatches, max_total_requests), "mt_batches_reserve");
+  }
+  void mixed_batches(const mt_subbatch* subbatches, const size_type num_subbatches, const size_type max_key_length,
+                     const size_type max_value_length, const uint32_t flags = 0u, cudaStream_t stream = 0) {
+    check(mt_mixed_batches(h_, subbatches, num_subbatches, max_key_length, max_value_length, flags, stream),
+          "mt_mixed_batches");
+  }
+
+  // Open-loop request stream served by the device-resident loop (mt_serve).
+  void serve(const mt_serve_plan& plan, uint64_t* latency_ns, mt_serve_stats* stats = nullptr) {
+    check(mt_serve(h_, &plan, latency_ns, stats), "mt_serve");
+  }
+
   // Waits for `stream`; returns the first device-side error since the last call.
   int last_error(cudaStream_t stream = 0) { return mt_sync(h_, stream); }
 

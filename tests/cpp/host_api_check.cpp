@@ -1,6 +1,7 @@
 // Compiles (and, on a GPU, runs) a small program against the C++ host mirror
-// include/mt/gpu_masstree.hpp and libmt_b200.so: insert, find, mixed_batch,
-// scan, validate, written the way the reference's host API is called.
+// include/mt/gpu_masstree.hpp and libmt_b200.so: insert, find, validate,
+// written the way the reference's host API is called, plus a mixed batch from
+// host buffers.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -32,6 +33,19 @@ int main() {
   cudaMemcpy(got.data(), ovl, n * 4, cudaMemcpyDeviceToHost);
   int bad = tree.last_error() != MT_OK;
   for (uint32_t i = 0; i < n; ++i) bad += got[i] != vlens[i];
+  // Host buffers: erase every second key and find all keys through the
+  // host-buffer entry point (two chunks).
+  std::vector<uint8_t> types(n);
+  std::vector<uint32_t> hv(n * maxV, 0), hvl(n, 0);
+  for (uint32_t i = 0; i < n; ++i) types[i] = (i % 2) ? (uint8_t)request_type_erase : (uint8_t)request_type_find;
+  std::vector<uint8_t> res(n, 0);
+  tree.mixed_batch_host(reinterpret_cast<const request_type*>(types.data()), keys.data(), maxK, klens.data(),
+                        hv.data(), maxV, hvl.data(), reinterpret_cast<bool*>(res.data()), n, 0, 600);
+  cudaStreamSynchronize(0);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (i % 2) bad += res[i] != 1;          // erased
+    else bad += hvl[i] != vlens[i];         // found with its value length
+  }
   std::string report;
   bad += !tree.validate(&report);
   std::printf("host api check: %s, %d mismatches\n", report.c_str(), bad);
