@@ -365,7 +365,8 @@ def run_ours(args, rank, world, dist):
                                    "after a 16M-key preload; keys 2-16 slices, 4096 shared prefixes; values 1-8 slices",
                        "preload_keys": args.preload, "batch_requests": args.batch, "max_key_length": MAXK,
                        "max_value_length": MAXV, "tile_size": args.tile, "write_tile_size": args.write_tile,
-                       "form": "plain per-call mixed_batch (partition, find pass, write pass)",
+                       "form": "plain per-call mixed_batch (reclaim, three-way partition, find / insert / "
+                               "update+erase class kernels on forked streams)",
                        "l2": "no flush: the index (>2 GB of slabs) and each batch's inputs exceed the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "batch_latency_ms": {"p50": round(sorted_steps[len(sorted_steps) // 2], 4),
@@ -379,10 +380,10 @@ def run_ours(args, rank, world, dist):
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": None if tr is None else int(tr * args.batch),
                          "algorithmic_bytes_per_step": abytes // args.steps,
-                         "kernel": "mixed_batch call: partition + find pass + write pass + reclaim"},
+                         "kernel": "mixed_batch call: reclaim + partition + three class kernels"},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": 5 * args.steps,  # reclaim, partition, find, insert, update/erase per step
             "pool": {"used_slabs": stats["used_slabs"], "total_slabs": stats["total_slabs"]},
         }
         res.update(extra)
