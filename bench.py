@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=1 << 20)
     ap.add_argument("--tile", type=int, default=8, help="lanes per find")
     ap.add_argument("--write-tile", type=int, default=32, help="lanes per insert/update/erase")
+    ap.add_argument("--scan-tile", type=int, default=4, help="lanes per scan query (c3 section)")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--bucket", type=int, default=0, help="1: mixed_batch serves short keys before long keys")
     ap.add_argument("--host-chunk", type=int, default=0,
@@ -605,6 +606,7 @@ def run_c3(args, stream, peak):
     oklens = torch.zeros((nq, mc), dtype=torch.uint32, device="cuda")
     with GpuMasstree(pool_bytes=8 << 30, tile_size=args.tile) as t:
         t.set_write_tile_size(args.write_tile)
+        t.set_scan_tile_size(args.scan_tile)
         step = 1 << 20
         for s0 in range(0, n, step):
             sl = slice(s0, s0 + step)

@@ -96,6 +96,10 @@ int mt_set_tile_size(mt_masstree* tree, uint32_t tile_size);
  * sets both widths). */
 int mt_set_write_tile_size(mt_masstree* tree, uint32_t tile_size);
 int mt_set_blocks_per_sm(mt_masstree* tree, uint32_t blocks_per_sm);
+/* Lanes per scan query (4/8/16/32; 0 = the find width, the default).  Scans
+ * read many independent suffix lines per query and run fastest with narrow
+ * tiles (more queries in flight).  New in this library. */
+int mt_set_scan_tile_size(mt_masstree* tree, uint32_t tile_size);
 
 /* Reference gpu_masstree::find (gpu_masstree.hpp:86-99). */
 int mt_find(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,

@@ -18,6 +18,7 @@ SIGNATURES = {
     "mt_set_tile_size": (_int, [_p, _u32]),
     "mt_set_write_tile_size": (_int, [_p, _u32]),
     "mt_set_blocks_per_sm": (_int, [_p, _u32]),
+    "mt_set_scan_tile_size": (_int, [_p, _u32]),
     "mt_find": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _u32, _p]),
     "mt_insert": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),
     "mt_update": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),

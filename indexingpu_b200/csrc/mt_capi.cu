@@ -393,7 +393,7 @@ int launch_scan_t(mt_masstree* t, scan_args a, cudaStream_t s) {
 
 template <bool CONC>
 int launch_scan(mt_masstree* t, const scan_args& a, cudaStream_t s) {
-  switch (t->tile_size) {
+  switch (t->scan_tile_size ? t->scan_tile_size : t->tile_size) {
     case 4: return launch_scan_t<4, CONC>(t, a, s);
     case 8: return launch_scan_t<8, CONC>(t, a, s);
     case 16: return launch_scan_t<16, CONC>(t, a, s);
@@ -503,6 +503,12 @@ int mt_set_tile_size(mt_masstree* t, uint32_t ts) {
 int mt_set_write_tile_size(mt_masstree* t, uint32_t ts) {
   if (!t || !valid_tile(ts)) return MT_ERR_INVALID_ARG;
   t->write_tile_size = ts;
+  return MT_OK;
+}
+
+int mt_set_scan_tile_size(mt_masstree* t, uint32_t ts) {
+  if (!t || (ts != 0 && !valid_tile(ts))) return MT_ERR_INVALID_ARG;
+  t->scan_tile_size = ts;
   return MT_OK;
 }
 

@@ -169,6 +169,7 @@ struct mt_masstree {
   int sms = 0;
   uint32_t tile_size = 8;        // finds and scans
   uint32_t write_tile_size = 8;  // inserts, updates, erases
+  uint32_t scan_tile_size = 0;   // scans (0: the find width)
   uint32_t blocks_per_sm = 0;    // 0 = occupancy limit
   uint32_t* split_idx = nullptr; // mixed-batch partition scratch
   uint32_t split_cap = 0;

@@ -97,6 +97,10 @@ class GpuMasstree:
     def set_write_tile_size(self, tile_size):
         self._check(self._lib.mt_set_write_tile_size(self._h, tile_size), "mt_set_write_tile_size")
 
+    def set_scan_tile_size(self, tile_size):
+        """Lanes per scan query (0: the find width)."""
+        self._check(self._lib.mt_set_scan_tile_size(self._h, tile_size), "mt_set_scan_tile_size")
+
     def set_blocks_per_sm(self, blocks_per_sm):
         self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
 

@@ -164,6 +164,26 @@ def test_c3_scan(tile):
         g.close()
 
 
+@pytest.mark.parametrize("scan_tile", [4, 32])
+def test_c3_scan_own_tile_width(scan_tile):
+    """Scans with their own tile width (mt_set_scan_tile_size) beside finds of
+    another: identical results to the oracle."""
+    w = wl.c3(50000, 3000)
+    g, o = GpuIndex(8), OracleIndex()
+    try:
+        g.t.set_scan_tile_size(scan_tile)
+        g.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        o.insert(w["keys"], w["lens"], w["vals"], w["vlens"])
+        rg = g.scan(w["lower"], w["lower_lens"], 100, maxV=1)
+        ro = o.scan(w["lower"], w["lower_lens"], 100, maxV=1)
+        for a, b, name in zip(rg, ro, ["counts", "values", "value_lengths", "keys", "key_lengths"]):
+            np.testing.assert_array_equal(a, b, err_msg=f"scan {name}")
+        gv, gl = g.find(w["keys"][:5000], w["lens"][:5000], 1)
+        np.testing.assert_array_equal(gl, np.ones(5000, np.uint32))
+    finally:
+        g.close()
+
+
 def test_scan_with_upper_varlen(tile):
     c2 = wl.C2(n_preload=30000, n_prefixes=16)
     keys, lens, vals, vlens = c2.keys(np.arange(30000))
