@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batch_kernel(tre
 }
 
 template <int T, bool CONC>
-__global__ void __launch_bounds__(kBlock) scan_kernel(tree_view tv, scan_args a) {
+__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) scan_kernel(tree_view tv, scan_args a) {
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
