@@ -143,7 +143,7 @@ def test_mixed_batches_graph_replay(persistent):
                 buf["vlens"].copy_(torch.from_numpy(vl))
             torch.cuda.synchronize()
 
-        # Warm-up call outside capture (first-call setup), on round 0's data.
+        # Warm-up call outside capture (first-call setup), on the first plan's data.
         load(plans[0])
         s = torch.cuda.Stream()
         with torch.cuda.stream(s):
