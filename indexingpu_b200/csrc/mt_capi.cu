@@ -462,6 +462,26 @@ int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
 
 }  // namespace
 
+namespace mtb {
+int host_launch_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s) {
+  return upsert ? launch_batch<OP_UPSERT, true>(t, a, s) : launch_batch<OP_INSERT, true>(t, a, s);
+}
+}  // namespace mtb
+
+namespace {
+// Whether the tree holds nothing: one slab in use (the root) and a root
+// without entries (waits for the device).
+bool tree_is_empty(mt_masstree* t) {
+  mt_stats_t st{};
+  if (mt_stats(t, &st) != MT_OK || st.used_slabs != 1u || st.limbo_slabs != 0u) return false;
+  uint32_t meta = 0;
+  if (cudaMemcpy(&meta, t->tv.pool.addr(t->tv.root) + WORD_META, sizeof(meta), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return false;
+  return (meta & META_COUNT) == 0u;
+}
+}  // namespace
+
 extern "C" {
 
 int mt_create(mt_masstree** out, float pool_ratio, uint32_t tile_size) {
@@ -535,8 +555,12 @@ int mt_insert(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_
   a.keys = keys; a.key_lengths = klens; a.values = const_cast<uint32_t*>(values); a.value_lengths_in = vlens;
   a.results = results; a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
   cudaStream_t s = (cudaStream_t)stream;
-  return (flags & MT_FLAG_UPDATE_IF_EXISTS) ? launch_batch<OP_UPSERT, true>(t, a, s)
-                                            : launch_batch<OP_INSERT, true>(t, a, s);
+  const bool upsert = (flags & MT_FLAG_UPDATE_IF_EXISTS) != 0;
+  if (n >= kBulkMin && tree_is_empty(t)) {
+    const int rc = host_bulk_insert(t, a, upsert, s);
+    if (rc != kBulkDeclined) return rc;
+  }
+  return upsert ? launch_batch<OP_UPSERT, true>(t, a, s) : launch_batch<OP_INSERT, true>(t, a, s);
 }
 
 int mt_update(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, const uint32_t* values,

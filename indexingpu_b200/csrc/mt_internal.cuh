@@ -197,6 +197,12 @@ int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
 int host_fork(mt_masstree* t, cudaStream_t s);
 int host_join(mt_masstree* t, cudaStream_t s, int rc);
 void host_pipe_free(mt_masstree* t);  // mt_host.cu
+int host_launch_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s);
+// Bulk build of a new tree's first layer (mt_bulk.cu): MT_OK, an error, or
+// kBulkDeclined when the batch does not suit it (insert it as usual).
+constexpr int kBulkDeclined = -1000;
+constexpr uint32_t kBulkMin = 1u << 16;  // smallest insert call that may bulk-build
+int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s);
 bool host_valid_tile(uint32_t ts);
 }  // namespace mtb
 
