@@ -275,7 +275,8 @@ int dalloc(X** p, size_t n) {
 namespace mtb {
 
 // Returns MT_OK after building (and inserting the rest), or kBulkDeclined when
-// the batch does not suit a bulk build (the caller inserts it as usual).
+// the batch does not suit a bulk build or its scratch does not fit in device
+// memory (the caller inserts it as usual).
 int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s) {
   const uint32_t n = a.n;
   bulk_view b{};
@@ -306,6 +307,20 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
   if (!rc) rc = dalloc(&highs[1], max_nodes);
   uint32_t* ids2 = nullptr;
   if (!rc) rc = dalloc(&ids2, max_nodes);
+  auto release = [&] {
+    for (void* q : {(void*)b.counts, (void*)b.offsets, (void*)b.ctl, (void*)b.order, (void*)b.rest,
+                    (void*)b.block_uniques, (void*)b.e_slice, (void*)b.e_val, (void*)b.e_state, (void*)b.e_src,
+                    (void*)ids, (void*)ids2, (void*)highs[0], (void*)highs[1]})
+      if (q) cudaFree(q);
+  };
+  if (rc) {
+    // No room for the scratch beside the slab pool: the ordinary insert needs
+    // none.  Clear the failed allocation's error so later launch checks do
+    // not report it.
+    cudaGetLastError();
+    release();
+    return kBulkDeclined;
+  }
   uint32_t h[4] = {0, 0, 0, 0};
   const int grid = std::max(1, t->sms * 8);
   if (!rc) rc = cu(cudaMemsetAsync(b.counts, 0, kBuckets * sizeof(uint32_t), s));
@@ -382,10 +397,7 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
     }
   }
   cudaStreamSynchronize(s);
-  for (void* q : {(void*)b.counts, (void*)b.offsets, (void*)b.ctl, (void*)b.order, (void*)b.rest,
-                  (void*)b.block_uniques, (void*)b.e_slice, (void*)b.e_val, (void*)b.e_state, (void*)b.e_src,
-                  (void*)ids, (void*)ids2, (void*)highs[0], (void*)highs[1]})
-    if (q) cudaFree(q);
+  release();
   if (rc) return rc;
   return declined ? kBulkDeclined : MT_OK;
 }
