@@ -108,6 +108,11 @@ class gpu_masstree {
 
   // ---- additions of this library (no counterpart in the reference) ----------
 
+  // Lanes per scan query (4/8/16/32; 0 = the find width).
+  void set_scan_tile_size(const size_type tile_size) {
+    check(mt_set_scan_tile_size(h_, tile_size), "mt_set_scan_tile_size");
+  }
+
   // mixed_batch with every buffer in pinned host memory; uploads, work and
   // downloads of consecutive chunks overlap (mt_mixed_batch_host).
   void mixed_batch_host(const request_type* request_types, const key_slice_type* keys,
