@@ -7,9 +7,12 @@
 //   * concurrent (find/scan): selects loads that tolerate concurrent writers;
 //   * update_if_exists (insert): upsert;
 //   * use_upper_key (scan): stop after the upper key;
-//   * enable_suffix, use_shmem_key and the erase merge switches are accepted
+//   * do_merge (erase) and erase_do_merge (mixed_batch): merge sparse border
+//     nodes after the call's erases (MT_FLAG_MERGE; space only, results are
+//     the same);
+//   * enable_suffix, use_shmem_key and the other erase switches are accepted
 //     and do not change results (this library always stores key tails in
-//     suffix chains and never merges nodes).
+//     suffix chains).
 // Device-side failures surface through last_error() (which synchronises the
 // stream) instead of std::terminate.
 #pragma once
@@ -78,7 +81,8 @@ class gpu_masstree {
             bool concurrent = true, bool use_shmem_key = false>
   void erase(const key_slice_type* keys, const size_type max_key_length, const size_type* key_lengths,
              const size_type num_keys, cudaStream_t stream = 0) {
-    check(mt_erase(h_, keys, max_key_length, key_lengths, num_keys, nullptr, 0u, stream), "mt_erase");
+    check(mt_erase(h_, keys, max_key_length, key_lengths, num_keys, nullptr, do_merge ? MT_FLAG_MERGE : 0u, stream),
+          "mt_erase");
   }
 
   template <bool use_upper_key = true, bool concurrent = false, bool use_shmem_key = false>
@@ -102,7 +106,8 @@ class gpu_masstree {
                    size_type* value_lengths, bool* results, const size_type num_requests,
                    cudaStream_t stream = 0) {
     check(mt_mixed_batch(h_, reinterpret_cast<const uint8_t*>(request_types), keys, max_key_length, key_lengths,
-                         values, max_value_length, value_lengths, results, num_requests, 0u, stream),
+                         values, max_value_length, value_lengths, results, num_requests,
+                         erase_do_merge ? MT_FLAG_MERGE : 0u, stream),
           "mt_mixed_batch");
   }
 

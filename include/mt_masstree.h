@@ -54,6 +54,10 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
                                        every request class */
 #define MT_FLAG_PERSISTENT 32u      /* mixed_batches: one cooperative persistent launch for all
                                        sub-batches instead of three class kernels per sub-batch */
+#define MT_FLAG_MERGE 64u           /* erase, mixed_batch: after the call's erases, fold border
+                                       nodes left with 4 entries or fewer into a neighbour under
+                                       the same parent (reference erase merge levels 2-4; space
+                                       only, results are the same) */
 
 /* One sub-batch of mt_mixed_batches: the buffers of one mt_mixed_batch call
  * (device pointers; max lengths are common to all sub-batches). */

@@ -12,8 +12,9 @@
 //                               (the reference accepts 16 or 32)
 //   lookup_concurrent (false)   find/scan loads that tolerate concurrent writers
 //   enable_suffix (true)        accepted; key tails always live in suffix chains
-//   merge_level (4)             0-4 accepted; erase never merges nodes, results
-//                               are the same at every level
+//   merge_level (4)             0-4; 2 and above merge sparse border nodes after
+//                               erases (MT_FLAG_MERGE), results are the same
+//                               at every level
 //   use_shmem_key (false)       accepted; no effect
 // and two of this library's own:
 //   write_tile_size (32)        lanes per insert/update/erase request
@@ -110,7 +111,11 @@ struct gpu_masstree_adapter {
     tree().update(keys, keylen_max, key_lengths, values, valuelen_max, value_lengths, count(num_keys));
   }
   void erase(const key_slice_type* keys, uint32_t keylen_max, const size_type* key_lengths, std::size_t num_keys) {
-    tree().erase(keys, keylen_max, key_lengths, count(num_keys));
+    if (configs_.merge_level >= 2) {
+      tree().erase<true, true, true>(keys, keylen_max, key_lengths, count(num_keys));
+    } else {
+      tree().erase<false, false, false>(keys, keylen_max, key_lengths, count(num_keys));
+    }
   }
   void find(const key_slice_type* keys, uint32_t keylen_max, const size_type* key_lengths,
             value_slice_type* results, uint32_t valuelen_max, size_type* result_lengths, std::size_t num_keys) {
@@ -141,8 +146,14 @@ struct gpu_masstree_adapter {
                    const size_type* key_lengths, value_slice_type* values, uint32_t valuelen_max,
                    size_type* value_lengths, std::size_t num_keys) {
     static_assert(sizeof(request_type) == 1, "request types are one byte");
-    tree().mixed_batch(reinterpret_cast<const GpuMasstreeB200::request_type*>(types), keys, keylen_max, key_lengths,
-                       values, valuelen_max, value_lengths, nullptr, count(num_keys));
+    const auto* rt = reinterpret_cast<const GpuMasstreeB200::request_type*>(types);
+    if (configs_.merge_level >= 2) {
+      tree().mixed_batch<true, true, true, true>(rt, keys, keylen_max, key_lengths, values, valuelen_max,
+                                                 value_lengths, nullptr, count(num_keys));
+    } else {
+      tree().mixed_batch<true, false, false, false>(rt, keys, keylen_max, key_lengths, values, valuelen_max,
+                                                    value_lengths, nullptr, count(num_keys));
+    }
   }
   void print_stats() {
     const mt_stats_t s = tree().stats();

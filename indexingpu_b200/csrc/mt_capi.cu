@@ -501,6 +501,7 @@ int mt_destroy(mt_masstree* t) {
   if (t->frames) cudaFree(t->frames);
   if (t->split_idx) cudaFree(t->split_idx);
   if (t->batches_mem) cudaFree(t->batches_mem);
+  if (t->merge_log) cudaFree(t->merge_log);
   host_pipe_free(t);
   if (t->mem) cudaFree(t->mem);
   if (t->h_err) cudaFreeHost(t->h_err);
@@ -575,11 +576,14 @@ int mt_update(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_
 
 int mt_erase(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, uint32_t n,
              bool* results, uint32_t flags, void* stream) {
-  (void)flags;
   if (!t || (n && (!keys || maxK == 0))) return MT_ERR_INVALID_ARG;
   batch_args a{};
   a.keys = keys; a.key_lengths = klens; a.results = results; a.max_key_length = maxK; a.n = n;
-  return launch_batch<OP_ERASE, true>(t, a, (cudaStream_t)stream);
+  const cudaStream_t s = (cudaStream_t)stream;
+  if (!(flags & MT_FLAG_MERGE)) return launch_batch<OP_ERASE, true>(t, a, s);
+  const int rc = host_merge_begin(t, s);
+  if (rc) return rc;
+  return host_merge_end(t, s, launch_batch<OP_ERASE, true>(t, a, s));
 }
 
 int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, uint32_t maxK,
@@ -590,8 +594,15 @@ int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, u
   a.types = types; a.keys = keys; a.key_lengths = klens; a.values = values;
   a.value_lengths_in = vlens; a.value_lengths_out = vlens; a.results = results;
   a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
-  if (flags & MT_FLAG_SINGLE_PASS) return launch_batch<OP_MIXED, true>(t, a, (cudaStream_t)stream);
-  return launch_mixed_split(t, a, (flags & MT_FLAG_BUCKET_KEYS) != 0, (cudaStream_t)stream);
+  const cudaStream_t s = (cudaStream_t)stream;
+  auto run = [&] {
+    if (flags & MT_FLAG_SINGLE_PASS) return launch_batch<OP_MIXED, true>(t, a, s);
+    return launch_mixed_split(t, a, (flags & MT_FLAG_BUCKET_KEYS) != 0, s);
+  };
+  if (!(flags & MT_FLAG_MERGE)) return run();
+  const int rc = host_merge_begin(t, s);
+  if (rc) return rc;
+  return host_merge_end(t, s, run());
 }
 
 int mt_scan(mt_masstree* t, const uint32_t* lower, const uint32_t* lower_lens, uint32_t maxK, uint32_t max_count,

@@ -306,6 +306,21 @@ struct node {
       w[k] = (g < lim) ? v : 0u;
     }
   }
+  // Append the entries of src (all greater than this node's) after this
+  // node's entries; the caller checks that both fit.
+  MT_DEV void append_from(const tile<T>& t, const node& src) {
+    const uint32_t a = count(), b = src.count();
+    const uint32_t sh = 2u * a;  // word g takes src word g - sh
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const uint32_t g = t.rank * W + k;
+      const uint32_t srcg = (g + 32u - sh) & 31u;
+      const uint32_t v = t.shfl(reg_select(src.w, (uint32_t)((k + W - (int)(sh % W)) % W)), (int)(srcg / W));
+      if (g >= sh && g < sh + 2u * b) w[k] = v;
+    }
+    ks = (ks | (src.ks << sh)) & 0x0FFFFFFFu;
+    meta = (meta & ~META_COUNT) | (a + b);
+  }
   // Keep entries [0, p): clear the entry words [2p, 26).
   MT_DEV void truncate(const tile<T>& t, uint32_t p) {
 #pragma unroll

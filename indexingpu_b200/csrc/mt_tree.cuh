@@ -51,7 +51,16 @@ enum op_result : int { RES_ERR = -1, RES_FAIL = 0, RES_OK = 1 };
 struct tree_view {
   pool_view pool;
   uint32_t root;  // root slab of trie layer 0 (never moves)
+  // Merge log of the current call, null unless the call merges sparse nodes
+  // after its erases: [0] records, [1] unused, then one (layer root, slice)
+  // pair per border node that an erase left with kMergeAt entries or none.
+  uint32_t* merge_log;
+  uint32_t merge_cap;
 };
+
+// A border node with this many entries or fewer after an erase is a merge
+// candidate (of kMaxEntries = 13).
+constexpr uint32_t kMergeAt = 4;
 
 // ---- locking -----------------------------------------------------------------
 
@@ -684,6 +693,13 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
     nd.remove_at(t, (uint32_t)e);
     publish_unlock(t, p, nd);
     if (st != KS_VALUE) suffix_retire<T, kConcSuffix>(t, p, v);
+    if (tv.merge_log != nullptr && t.leader() && !nd.is_root() && (nd.count() == kMergeAt || nd.count() == 0u)) {
+      const uint32_t r = atomicAdd(tv.merge_log, 1u);
+      if (r < tv.merge_cap) {
+        tv.merge_log[2u + 2u * r] = root;
+        tv.merge_log[3u + 2u * r] = slice;
+      }
+    }
     return RES_OK;
   }
   return RES_FAIL;

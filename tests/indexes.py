@@ -128,12 +128,12 @@ class GpuIndex(_TorchIndex):
         self.t.sync()
         return self.h(res).astype(np.uint8)
 
-    def erase(self, keys, klens, n=None):
+    def erase(self, keys, klens, n=None, merge=False):
         torch = self.torch
         keys = _u32(keys)
         n = len(keys) if n is None else n
         res = self.zeros(n, torch.bool)
-        self.t.erase(self.d(keys), keys.shape[1], self.d(_u32(klens)), n, results=res)
+        self.t.erase(self.d(keys), keys.shape[1], self.d(_u32(klens)), n, results=res, merge=merge)
         self.t.sync()
         return self.h(res).astype(np.uint8)
 
@@ -147,7 +147,7 @@ class GpuIndex(_TorchIndex):
         self.t.sync()
         return self.h(vals), self.h(vlens)
 
-    def mixed(self, types, keys, klens, vals, vlens, n=None, bucket_keys=False):
+    def mixed(self, types, keys, klens, vals, vlens, n=None, bucket_keys=False, merge=False):
         torch = self.torch
         keys = _u32(keys)
         n = len(keys) if n is None else n
@@ -155,7 +155,7 @@ class GpuIndex(_TorchIndex):
         dvl = self.d(_u32(vlens))
         res = self.zeros(n, torch.bool)
         self.t.mixed_batch(self.d(np.ascontiguousarray(types, np.uint8)), self.d(keys), keys.shape[1],
-                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n, bucket_keys=bucket_keys)
+                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n, bucket_keys=bucket_keys, merge=merge)
         self.t.sync()
         return self.h(dv), self.h(dvl), self.h(res).astype(np.uint8)
 
@@ -175,3 +175,32 @@ class GpuIndex(_TorchIndex):
                     oklens, concurrent=concurrent)
         self.t.sync()
         return self.h(counts), self.h(vals), self.h(vlens), self.h(okeys), self.h(oklens)
+
+
+def dump_by_scan(g, maxK, maxV, n):
+    """Every (key, key length, value, value length) of a GpuIndex in key order,
+    by one scan from the smallest key."""
+    import torch
+    t = g.t
+    lower = torch.zeros((1, maxK), dtype=torch.uint32, device="cuda")
+    lens = torch.ones(1, dtype=torch.uint32, device="cuda")
+    counts = torch.zeros(1, dtype=torch.uint32, device="cuda")
+    vals = torch.zeros((1, n, maxV), dtype=torch.uint32, device="cuda")
+    vlens = torch.zeros((1, n), dtype=torch.uint32, device="cuda")
+    keys = torch.zeros((1, n, maxK), dtype=torch.uint32, device="cuda")
+    klens = torch.zeros((1, n), dtype=torch.uint32, device="cuda")
+    t.scan(lower, lens, maxK, n, 1, counts=counts, values=vals, max_value_length=maxV, value_lengths=vlens,
+           out_keys=keys, out_key_lengths=klens)
+    t.sync()
+    c = int(counts[0])
+    return [x[0, :c].cpu().numpy() for x in (keys, klens, vals, vlens)]
+
+
+def same_state(g, o, maxK, maxV):
+    """The GpuIndex holds exactly the oracle's keys and values."""
+    n = o.o.size()
+    a = dump_by_scan(g, maxK, maxV, n + 8)
+    b = o.dump(maxK, maxV)
+    assert len(a[0]) == n
+    for x, y, name in zip(a, b, ["keys", "key lengths", "values", "value lengths"]):
+        np.testing.assert_array_equal(x, y, err_msg=name)

@@ -5,37 +5,11 @@ must validate, and it must keep working under ordinary mixed batches."""
 import numpy as np
 import pytest
 
-from indexes import GpuIndex, OracleIndex
+from indexes import GpuIndex, OracleIndex, same_state
 from indexingpu_b200 import workload as wl
 from scenarios import assert_found
 
 pytestmark = pytest.mark.gpu
-
-
-def _dump(g, maxK, maxV, n):
-    import torch
-    t = g.t
-    lower = torch.zeros((1, maxK), dtype=torch.uint32, device="cuda")
-    lens = torch.ones(1, dtype=torch.uint32, device="cuda")
-    counts = torch.zeros(1, dtype=torch.uint32, device="cuda")
-    vals = torch.zeros((1, n, maxV), dtype=torch.uint32, device="cuda")
-    vlens = torch.zeros((1, n), dtype=torch.uint32, device="cuda")
-    keys = torch.zeros((1, n, maxK), dtype=torch.uint32, device="cuda")
-    klens = torch.zeros((1, n), dtype=torch.uint32, device="cuda")
-    t.scan(lower, lens, maxK, n, 1, counts=counts, values=vals, max_value_length=maxV, value_lengths=vlens,
-           out_keys=keys, out_key_lengths=klens)
-    t.sync()
-    c = int(counts[0])
-    return [x[0, :c].cpu().numpy() for x in (keys, klens, vals, vlens)]
-
-
-def _same_state(g, o, maxK, maxV):
-    n = o.o.size()
-    a = _dump(g, maxK, maxV, n + 8)
-    b = o.dump(maxK, maxV)
-    assert len(a[0]) == n
-    for x, y, name in zip(a, b, ["keys", "key lengths", "values", "value lengths"]):
-        np.testing.assert_array_equal(x, y, err_msg=name)
 
 
 @pytest.mark.parametrize("tile", [8, 32])
@@ -54,7 +28,7 @@ def test_bulk_build_c1(tile):
         ok, nkeys, report = g.t.validate()
         assert ok, report
         assert nkeys == 200000
-        _same_state(g, o, 8, 2)
+        same_state(g, o, 8, 2)
     finally:
         g.close()
 
@@ -94,7 +68,7 @@ def test_bulk_build_duplicates_and_shared_slices(upsert):
         assert int(gr.sum()) == int(orr.sum())
         ok, nkeys, report = g.t.validate()
         assert ok, report
-        _same_state(g, o, maxK, maxV)
+        same_state(g, o, maxK, maxV)
     finally:
         g.close()
 
@@ -129,7 +103,7 @@ def test_bulk_built_tree_takes_mixed_batches():
             assert_found(gv[~nf], gl[~nf], ov[~nf], ol[~nf], "mixed finds")
         ok, _, report = g.t.validate()
         assert ok, report
-        _same_state(g, o, 8, 2)
+        same_state(g, o, 8, 2)
     finally:
         g.close()
 

@@ -1,0 +1,107 @@
+"""Erase with MT_FLAG_MERGE (the reference's erase merge levels 2-4): sparse
+border nodes are folded into a neighbour after the call's erases.  Results and
+the full ordered contents must equal the oracle's and the tree must validate,
+through later inserts, finds and mixed batches too; the merged tree must hold
+fewer slabs than the same tree erased without merges."""
+import numpy as np
+import pytest
+
+from indexes import GpuIndex, OracleIndex, same_state
+from indexingpu_b200 import workload as wl
+from scenarios import assert_found
+
+pytestmark = pytest.mark.gpu
+
+
+def _used(g):
+    return g.t.stats()["used_slabs"]
+
+
+@pytest.mark.parametrize("bulk", [True, False])
+@pytest.mark.parametrize("write_tile", [8, 32])
+def test_merge_after_erase_c1(bulk, write_tile):
+    """C1 keys: 80% erased in two calls, with and without merges; then the
+    erased keys inserted again."""
+    n = 200000
+    d = wl.c1(n_keys=n, n_finds=1000)
+    keys, lens, vals, vlens = d["keys"], d["lens"], d["vals"], d["vlens"]
+    gm, g0, o = GpuIndex(tile_size=8, pool_bytes=1 << 30), GpuIndex(tile_size=8, pool_bytes=1 << 30), OracleIndex()
+    try:
+        for g in (gm, g0):
+            g.t.set_write_tile_size(write_tile)
+            # One call takes the bulk build (packed nodes); chunks below its
+            # minimum grow the tree by splits (half-full nodes).
+            step = n if bulk else 40000
+            for a in range(0, n, step):
+                g.insert(keys[a:a + step], lens[a:a + step], vals[a:a + step], vlens[a:a + step])
+        o.insert(keys, lens, vals, vlens)
+        rng = np.random.default_rng(5)
+        gone = rng.permutation(n)[: n * 8 // 10]
+        for part in np.array_split(gone, 2):
+            rm = gm.erase(keys[part], lens[part], merge=True)
+            r0 = g0.erase(keys[part], lens[part])
+            ro = o.erase(keys[part], lens[part])
+            np.testing.assert_array_equal(rm, ro)
+            np.testing.assert_array_equal(r0, ro)
+        for g in (gm, g0):
+            ok, nkeys, report = g.t.validate()
+            assert ok, report
+            assert nkeys == n - len(gone)
+        same_state(gm, o, 8, 2)
+        assert _used(gm) < 0.9 * _used(g0), (_used(gm), _used(g0))
+        # Finds of everything, then the erased keys back in.
+        gv, gl = gm.find(keys, lens, 2)
+        ov, ol = o.find(keys, lens, 2)
+        assert_found(gv, gl, ov, ol, "finds on the merged tree")
+        np.testing.assert_array_equal(gm.insert(keys[gone], lens[gone], vals[gone], vlens[gone]),
+                                      o.insert(keys[gone], lens[gone], vals[gone], vlens[gone]))
+        ok, nkeys, report = gm.t.validate()
+        assert ok, report
+        assert nkeys == n
+        same_state(gm, o, 8, 2)
+    finally:
+        gm.close()
+        g0.close()
+
+
+def test_merge_in_mixed_batches_c2():
+    """C2 keys (shared prefixes, several trie layers): touch-once mixed batches
+    that erase most of the tree with merges on, plus finds and inserts."""
+    c2 = wl.C2(n_preload=120000, n_prefixes=64)
+    keys, lens, vals, vlens = c2.keys(np.arange(120000))
+    g, o = GpuIndex(tile_size=8, pool_bytes=1 << 30), OracleIndex()
+    try:
+        g.insert(keys, lens, vals, vlens)
+        o.insert(keys, lens, vals, vlens)
+        rng = np.random.default_rng(9)
+        order = rng.permutation(120000)
+        fresh = 120000
+        for b in range(3):
+            # 30,000 present keys per batch: 80% erased, 20% found; plus 2,000
+            # new keys inserted.
+            pick = order[b * 30000:(b + 1) * 30000]
+            types = np.where(rng.random(30000) < 0.8, wl.REQ_ERASE, wl.REQ_FIND).astype(np.uint8)
+            nk, nl, nv, nvl = c2.keys(np.arange(fresh, fresh + 2000))
+            fresh += 2000
+            types = np.concatenate([types, np.full(2000, wl.REQ_INSERT, np.uint8)])
+            k = np.concatenate([keys[pick], nk])
+            ln = np.concatenate([lens[pick], nl])
+            v = np.concatenate([vals[pick], nv])
+            vl = np.concatenate([np.where(types[:30000] == wl.REQ_FIND, 0, vlens[pick]), nvl]).astype(np.uint32)
+            gv, gl, gr = g.mixed(types, k, ln, v, vl, merge=True)
+            ov, ol, orr = o.mixed(types, k, ln, v, vl)
+            nf = types != wl.REQ_FIND
+            np.testing.assert_array_equal(gr[nf], orr[nf])
+            assert_found(gv[~nf], gl[~nf], ov[~nf], ol[~nf], "mixed finds")
+            ok, _, report = g.t.validate()
+            assert ok, report
+        same_state(g, o, c2.maxK, c2.maxV)
+        # The rest erased through mt_erase with merges: layers emptied too.
+        rest = order[90000:]
+        np.testing.assert_array_equal(g.erase(keys[rest], lens[rest], merge=True), o.erase(keys[rest], lens[rest]))
+        ok, nkeys, report = g.t.validate()
+        assert ok, report
+        assert nkeys == o.o.size()
+        same_state(g, o, c2.maxK, c2.maxV)
+    finally:
+        g.close()
