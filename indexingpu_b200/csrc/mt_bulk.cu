@@ -30,7 +30,8 @@ struct bulk_view {
   uint32_t max_key_length, max_value_length, n;
   uint32_t* counts;          // [kBuckets] keys per bucket, then fill cursors
   uint32_t* offsets;         // [kBuckets] first position of every bucket
-  uint32_t* ctl;             // [0] valid keys, [1] largest bucket, [2] rest count, [3] unique count
+  uint32_t* ctl;             // [0] valid keys, [1] largest bucket, [2] rest count, [3] unique count,
+                             // [4] buckets holding keys
   unsigned long long* order; // [n] (first slice << 32 | request) in key order
   uint32_t* rest;            // [n] requests left to the ordinary insert
   uint32_t* block_uniques;   // [blocks of the classify pass] unique keys per block, then their offsets
@@ -54,6 +55,7 @@ __global__ void bulk_count_kernel(bulk_view b) {
     }
     const uint32_t bucket = b.keys[(size_t)i * b.max_key_length] >> 16;
     const uint32_t c = atomicAdd(&b.counts[bucket], 1u) + 1u;
+    if (c == 1u) atomicAdd(&b.ctl[4], 1u);
     atomicMax(&b.ctl[1], c);
     atomicAdd(&b.ctl[0], 1u);
   }
@@ -321,7 +323,7 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
     release();
     return kBulkDeclined;
   }
-  uint32_t h[4] = {0, 0, 0, 0};
+  uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int grid = std::max(1, t->sms * 8);
   if (!rc) rc = cu(cudaMemsetAsync(b.counts, 0, kBuckets * sizeof(uint32_t), s));
   if (!rc) rc = cu(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(uint32_t), s));
@@ -332,9 +334,10 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
   if (!rc) rc = cu(cudaMemcpyAsync(h, b.ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
   if (!rc) rc = cu(cudaStreamSynchronize(s));
   const uint32_t m = h[0];
-  // Decline when one bucket is large (keys sharing first slices: little to
-  // build, and the in-bucket sort would be slow).
-  bool declined = !rc && (h[1] > 2048u || m < n / 2u);
+  // Decline when one bucket is large, or the keys crowd into few buckets
+  // (first slices shared by many keys: little to build, and the in-bucket
+  // sort would be slow), or fewer than half the keys are valid.
+  bool declined = !rc && (h[1] > 2048u || h[4] < m / 64u || m < n / 2u);
   if (!rc && !declined) {
     bulk_scan_kernel<<<1, 1024, 0, s>>>(b);
     bulk_scatter_kernel<<<grid, 256, 0, s>>>(b);
