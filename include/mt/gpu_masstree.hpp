@@ -10,6 +10,10 @@
 //   * do_merge (erase) and erase_do_merge (mixed_batch): merge sparse border
 //     nodes after the call's erases (MT_FLAG_MERGE; space only, results are
 //     the same);
+//   * do_remove_empty_root (erase) and erase_do_remove_empty_root
+//     (mixed_batch), together with the merge switch as the reference requires:
+//     remove the trie layers that the call's erases empty
+//     (MT_FLAG_REMOVE_EMPTY_LAYERS; space only, results are the same);
 //   * enable_suffix, use_shmem_key and the other erase switches are accepted
 //     and do not change results (this library always stores key tails in
 //     suffix chains).
@@ -81,8 +85,9 @@ class gpu_masstree {
             bool concurrent = true, bool use_shmem_key = false>
   void erase(const key_slice_type* keys, const size_type max_key_length, const size_type* key_lengths,
              const size_type num_keys, cudaStream_t stream = 0) {
-    check(mt_erase(h_, keys, max_key_length, key_lengths, num_keys, nullptr, do_merge ? MT_FLAG_MERGE : 0u, stream),
-          "mt_erase");
+    const uint32_t flags =
+        (do_merge ? MT_FLAG_MERGE : 0u) | (do_merge && do_remove_empty_root ? MT_FLAG_REMOVE_EMPTY_LAYERS : 0u);
+    check(mt_erase(h_, keys, max_key_length, key_lengths, num_keys, nullptr, flags, stream), "mt_erase");
   }
 
   template <bool use_upper_key = true, bool concurrent = false, bool use_shmem_key = false>
@@ -107,7 +112,9 @@ class gpu_masstree {
                    cudaStream_t stream = 0) {
     check(mt_mixed_batch(h_, reinterpret_cast<const uint8_t*>(request_types), keys, max_key_length, key_lengths,
                          values, max_value_length, value_lengths, results, num_requests,
-                         erase_do_merge ? MT_FLAG_MERGE : 0u, stream),
+                         (erase_do_merge ? MT_FLAG_MERGE : 0u) |
+                             (erase_do_merge && erase_do_remove_empty_root ? MT_FLAG_REMOVE_EMPTY_LAYERS : 0u),
+                         stream),
           "mt_mixed_batch");
   }
 

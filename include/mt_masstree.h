@@ -58,6 +58,12 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
                                        nodes left with 4 entries or fewer into a neighbour under
                                        the same parent (reference erase merge levels 2-4; space
                                        only, results are the same) */
+#define MT_FLAG_REMOVE_EMPTY_LAYERS 128u /* erase, mixed_batch: after the call's erases (and merges),
+                                       remove every trie layer (1 or deeper, reached by at most 15
+                                       key slices) whose only node they left empty, and the parent
+                                       layers this empties in turn (reference erase merge level 4,
+                                       do_remove_empty_root, include/gpu_masstree.hpp:914-960;
+                                       space only, results are the same) */
 
 /* One sub-batch of mt_mixed_batches: the buffers of one mt_mixed_batch call
  * (device pointers; max lengths are common to all sub-batches). */

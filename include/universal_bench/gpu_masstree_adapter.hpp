@@ -13,8 +13,9 @@
 //   lookup_concurrent (false)   find/scan loads that tolerate concurrent writers
 //   enable_suffix (true)        accepted; key tails always live in suffix chains
 //   merge_level (4)             0-4; 2 and above merge sparse border nodes after
-//                               erases (MT_FLAG_MERGE), results are the same
-//                               at every level
+//                               erases (MT_FLAG_MERGE), 4 also removes the trie
+//                               layers they empty (MT_FLAG_REMOVE_EMPTY_LAYERS);
+//                               results are the same at every level
 //   use_shmem_key (false)       accepted; no effect
 // and two of this library's own:
 //   write_tile_size (32)        lanes per insert/update/erase request
@@ -111,8 +112,10 @@ struct gpu_masstree_adapter {
     tree().update(keys, keylen_max, key_lengths, values, valuelen_max, value_lengths, count(num_keys));
   }
   void erase(const key_slice_type* keys, uint32_t keylen_max, const size_type* key_lengths, std::size_t num_keys) {
-    if (configs_.merge_level >= 2) {
+    if (configs_.merge_level >= 4) {
       tree().erase<true, true, true>(keys, keylen_max, key_lengths, count(num_keys));
+    } else if (configs_.merge_level >= 2) {
+      tree().erase<false, true, true>(keys, keylen_max, key_lengths, count(num_keys));
     } else {
       tree().erase<false, false, false>(keys, keylen_max, key_lengths, count(num_keys));
     }
@@ -147,9 +150,12 @@ struct gpu_masstree_adapter {
                    size_type* value_lengths, std::size_t num_keys) {
     static_assert(sizeof(request_type) == 1, "request types are one byte");
     const auto* rt = reinterpret_cast<const GpuMasstreeB200::request_type*>(types);
-    if (configs_.merge_level >= 2) {
+    if (configs_.merge_level >= 4) {
       tree().mixed_batch<true, true, true, true>(rt, keys, keylen_max, key_lengths, values, valuelen_max,
                                                  value_lengths, nullptr, count(num_keys));
+    } else if (configs_.merge_level >= 2) {
+      tree().mixed_batch<true, false, true, true>(rt, keys, keylen_max, key_lengths, values, valuelen_max,
+                                                  value_lengths, nullptr, count(num_keys));
     } else {
       tree().mixed_batch<true, false, false, false>(rt, keys, keylen_max, key_lengths, values, valuelen_max,
                                                     value_lengths, nullptr, count(num_keys));

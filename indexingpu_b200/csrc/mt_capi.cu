@@ -502,6 +502,7 @@ int mt_destroy(mt_masstree* t) {
   if (t->split_idx) cudaFree(t->split_idx);
   if (t->batches_mem) cudaFree(t->batches_mem);
   if (t->merge_log) cudaFree(t->merge_log);
+  if (t->layer_log) cudaFree(t->layer_log);
   host_pipe_free(t);
   if (t->mem) cudaFree(t->mem);
   if (t->h_err) cudaFreeHost(t->h_err);
@@ -580,8 +581,8 @@ int mt_erase(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t
   batch_args a{};
   a.keys = keys; a.key_lengths = klens; a.results = results; a.max_key_length = maxK; a.n = n;
   const cudaStream_t s = (cudaStream_t)stream;
-  if (!(flags & MT_FLAG_MERGE)) return launch_batch<OP_ERASE, true>(t, a, s);
-  const int rc = host_merge_begin(t, s);
+  if (!(flags & (MT_FLAG_MERGE | MT_FLAG_REMOVE_EMPTY_LAYERS))) return launch_batch<OP_ERASE, true>(t, a, s);
+  const int rc = host_merge_begin(t, s, flags);
   if (rc) return rc;
   return host_merge_end(t, s, launch_batch<OP_ERASE, true>(t, a, s));
 }
@@ -599,8 +600,8 @@ int mt_mixed_batch(mt_masstree* t, const uint8_t* types, const uint32_t* keys, u
     if (flags & MT_FLAG_SINGLE_PASS) return launch_batch<OP_MIXED, true>(t, a, s);
     return launch_mixed_split(t, a, (flags & MT_FLAG_BUCKET_KEYS) != 0, s);
   };
-  if (!(flags & MT_FLAG_MERGE)) return run();
-  const int rc = host_merge_begin(t, s);
+  if (!(flags & (MT_FLAG_MERGE | MT_FLAG_REMOVE_EMPTY_LAYERS))) return run();
+  const int rc = host_merge_begin(t, s, flags);
   if (rc) return rc;
   return host_merge_end(t, s, run());
 }

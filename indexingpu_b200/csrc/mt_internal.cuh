@@ -188,14 +188,17 @@ struct mt_masstree {
   void* batches_mem = nullptr;
   uint32_t batches_max_sub = 0;
   uint64_t batches_max_total = 0;
-  // Merge log of MT_FLAG_MERGE calls (see mt_merge.cu; created on first use).
+  // Merge log of MT_FLAG_MERGE calls and layer log of
+  // MT_FLAG_REMOVE_EMPTY_LAYERS calls (see mt_merge.cu; created on first use).
   uint32_t* merge_log = nullptr;
+  uint32_t* layer_log = nullptr;
 };
 
 namespace mtb {
-// MT_FLAG_MERGE (mt_merge.cu): begin logs the call's sparse border nodes,
-// end (given the call's status) merges them after the call's erase kernels.
-int host_merge_begin(mt_masstree* t, cudaStream_t s);
+// MT_FLAG_MERGE and MT_FLAG_REMOVE_EMPTY_LAYERS (mt_merge.cu): begin logs the
+// call's sparse border nodes and emptied layers as `flags` ask, end (given the
+// call's status) merges and removes them after the call's erase kernels.
+int host_merge_begin(mt_masstree* t, cudaStream_t s, uint32_t flags);
 int host_merge_end(mt_masstree* t, cudaStream_t s, int rc);
 // Host helpers implemented in mt_capi.cu.
 int host_max_blocks_per_sm(const void* fn, int block, size_t smem);

@@ -12,6 +12,16 @@
 // Child 0 of a parent is never the slab given up, so the sibling links that
 // cross parents stay valid.  Results never change, only space: a node merged
 // away holds no key that its neighbour does not now hold.
+//
+// Removal of emptied trie layers (MT_FLAG_REMOVE_EMPTY_LAYERS; the reference's
+// erase<do_remove_empty_root>, include/gpu_masstree.hpp:914-960).  An erase
+// that leaves the only node of a layer (1 or deeper) without entries logs the
+// key's slices above that layer.  After the call's erases (and merges) a pass
+// follows those slices to the border node that holds the layer's LINK entry,
+// locks it, locks the layer root, and when the root is still an empty border
+// node without siblings removes the LINK entry and retires the root; a parent
+// layer that this empties is removed in turn.  Locks are taken from the
+// shallower layer to the deeper one, so records of one pass cannot deadlock.
 #include <algorithm>
 
 #include "mt_internal.cuh"
@@ -136,30 +146,97 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) merge_kernel(tre
   }
 }
 
+// Remove the layer that record `rec` names, then every layer above it that the
+// removal leaves without entries.
+MT_DEV void remove_layers(const tile<32>& t, const tree_view& tv, const uint32_t* rec) {
+  const pool_view& p = tv.pool;
+  node<32> nd, cn;
+  for (uint32_t depth = rec[0]; depth >= 1u && depth < kLayerRecWords; --depth) {
+    // The root of layer depth-1, through the LINK entries of the slices above.
+    uint32_t root = tv.root, hops = 0;
+    for (uint32_t layer = 0; layer + 1u < depth; ++layer) {
+      if (!descend<32, kConc>(t, p, root, rec[1u + layer], nd, hops)) return;
+      const int e = nd.match(t, rec[1u + layer], true);
+      if (e < 0 || ks_get(nd.ks, (uint32_t)e) != KS_LINK) return;  // removed by an earlier record
+      root = nd.val_at(t, (uint32_t)e);
+    }
+    const uint32_t slice = rec[depth];
+    if (!descend<32, kConc>(t, p, root, slice, nd, hops) || !lock_border(t, p, slice, nd, hops)) return;
+    const int e = nd.match(t, slice, true);
+    if (e < 0 || ks_get(nd.ks, (uint32_t)e) != KS_LINK) {
+      unlock_node(t, p, nd.idx);
+      return;
+    }
+    const uint32_t child = nd.val_at(t, (uint32_t)e);
+    if (!p.valid(child) || !lock_load(t, p, child, cn)) {
+      if (!p.valid(child) && t.leader()) record_error(p, ERR_CORRUPT);
+      unlock_node(t, p, nd.idx);
+      return;
+    }
+    if (!cn.is_border() || !cn.is_root() || cn.has_sib() || cn.count() != 0u) {  // refilled or split since
+      unlock_node(t, p, child);
+      unlock_node(t, p, nd.idx);
+      return;
+    }
+    nd.remove_at(t, (uint32_t)e);
+    publish_unlock(t, p, nd);
+    unlock_node(t, p, child);
+    if (t.leader()) retire_slab(p, child);
+    if (!nd.is_root() || nd.count() != 0u || nd.has_sib()) return;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) remove_layers_kernel(tree_view tv,
+                                                                                      const uint32_t* log,
+                                                                                      uint32_t cap) {
+  tile<32> t;
+  const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const uint32_t num_tiles = (gridDim.x * blockDim.x) / 32u;
+  const uint32_t n = min(log[0], cap);
+  for (uint32_t r = tile_id; r < n; r += num_tiles) {
+    if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
+    remove_layers(t, tv, log + 2u + (size_t)kLayerRecWords * r);
+  }
+}
+
+constexpr uint32_t kLayerCap = 1u << 18;  // layer-log records per call (later ones are dropped)
+
+// Creates a log on first use; false when it does not fit beside the slab pool.
+bool ensure_log(uint32_t*& log, size_t words) {
+  if (log) return true;
+  if (cudaMalloc(reinterpret_cast<void**>(&log), words * sizeof(uint32_t)) == cudaSuccess) return true;
+  cudaGetLastError();
+  log = nullptr;
+  return false;
+}
+
 }  // namespace
 
-int host_merge_begin(mt_masstree* t, cudaStream_t s) {
-  if (!t->merge_log) {
-    if (cudaMalloc(reinterpret_cast<void**>(&t->merge_log), (2u + 2u * (size_t)kMergeCap) * sizeof(uint32_t)) !=
-        cudaSuccess) {
-      // No room beside the slab pool: the call erases without merging.
-      cudaGetLastError();
-      t->merge_log = nullptr;
-      return MT_OK;
-    }
+int host_merge_begin(mt_masstree* t, cudaStream_t s, uint32_t flags) {
+  // A log that does not fit beside the slab pool leaves the call erasing
+  // without that pass.
+  if ((flags & MT_FLAG_MERGE) && ensure_log(t->merge_log, 2u + 2u * (size_t)kMergeCap)) {
+    if (cudaMemsetAsync(t->merge_log, 0, 2u * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+    t->tv.merge_log = t->merge_log;
+    t->tv.merge_cap = kMergeCap;
   }
-  if (cudaMemsetAsync(t->merge_log, 0, 2u * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
-  t->tv.merge_log = t->merge_log;
-  t->tv.merge_cap = kMergeCap;
+  if ((flags & MT_FLAG_REMOVE_EMPTY_LAYERS) && ensure_log(t->layer_log, 2u + (size_t)kLayerRecWords * kLayerCap)) {
+    if (cudaMemsetAsync(t->layer_log, 0, 2u * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+    t->tv.layer_log = t->layer_log;
+    t->tv.layer_cap = kLayerCap;
+  }
   return MT_OK;
 }
 
 int host_merge_end(mt_masstree* t, cudaStream_t s, int rc) {
-  const bool logged = t->tv.merge_log != nullptr;
+  const bool merges = t->tv.merge_log != nullptr, layers = t->tv.layer_log != nullptr;
   t->tv.merge_log = nullptr;
   t->tv.merge_cap = 0;
-  if (rc != MT_OK || !logged) return rc;
-  merge_kernel<<<std::max(1, t->sms * 4), kBlock, 0, s>>>(t->tv, t->merge_log, kMergeCap);
+  t->tv.layer_log = nullptr;
+  t->tv.layer_cap = 0;
+  if (rc != MT_OK) return rc;
+  if (merges) merge_kernel<<<std::max(1, t->sms * 4), kBlock, 0, s>>>(t->tv, t->merge_log, kMergeCap);
+  if (layers) remove_layers_kernel<<<std::max(1, t->sms * 4), kBlock, 0, s>>>(t->tv, t->layer_log, kLayerCap);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
 }
 

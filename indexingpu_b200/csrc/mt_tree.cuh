@@ -22,8 +22,10 @@
 // split full nodes top-down on the way to the border node (the proactive
 // B-link split of Awad et al., "Engineering a High-Performance GPU B-Tree",
 // PPoPP 2019, which the reference also uses, include/gpu_masstree.hpp:1020-1148).
-// Erase removes entries without merging nodes (the reference's merge_level 0):
-// results are identical, empty nodes stay linked.  Every spin and every retry
+// Erase removes entries without merging nodes (the reference's merge_level 0);
+// on request it logs sparse border nodes and emptied trie layers, which a pass
+// after the call merges or removes (mt_merge.cu).  Results are the same either
+// way; only the space differs.  Every spin and every retry
 // loop is bounded and records an error code instead of hanging.
 #pragma once
 #include "mt_suffix.cuh"
@@ -56,7 +58,17 @@ struct tree_view {
   // pair per border node that an erase left with kMergeAt entries or none.
   uint32_t* merge_log;
   uint32_t merge_cap;
+  // Layer log of the current call, null unless the call removes the trie
+  // layers that its erases empty: [0] records, [1] unused, then records of
+  // kLayerRecWords words, {layer, key slices 0 .. layer-1}, one per erase
+  // that left the only node of a layer (layer 1 or deeper) without entries.
+  uint32_t* layer_log;
+  uint32_t layer_cap;
 };
+
+// Words per layer-log record; layers deeper than kLayerRecWords-1 are not
+// logged (and so never removed; the space stays in use, results are the same).
+constexpr uint32_t kLayerRecWords = 16;
 
 // A border node with this many entries or fewer after an erase is a merge
 // candidate (of kMaxEntries = 13).
@@ -698,6 +710,15 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
       if (r < tv.merge_cap) {
         tv.merge_log[2u + 2u * r] = root;
         tv.merge_log[3u + 2u * r] = slice;
+      }
+    }
+    if (tv.layer_log != nullptr && t.leader() && layer >= 1u && layer < kLayerRecWords && nd.is_root() &&
+        nd.count() == 0u && !nd.has_sib()) {
+      const uint32_t r = atomicAdd(tv.layer_log, 1u);
+      if (r < tv.layer_cap) {
+        uint32_t* rec = tv.layer_log + 2u + (size_t)kLayerRecWords * r;
+        rec[0] = layer;
+        for (uint32_t i = 0; i < layer; ++i) rec[1u + i] = key[i];
       }
     }
     return RES_OK;

@@ -29,6 +29,7 @@ REQ_INSERT, REQ_ERASE, REQ_FIND, REQ_UPDATE = 0, 1, 2, 3
 FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS, FLAG_BUCKET_KEYS = 1, 2, 4, 8, 16
 FLAG_PERSISTENT = 32
 FLAG_MERGE = 64
+FLAG_REMOVE_EMPTY_LAYERS = 128
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
@@ -127,9 +128,11 @@ class GpuMasstree:
                                  _stream(stream))
         self._check(rc, "mt_update")
 
-    def erase(self, keys, max_key_length, key_lengths, num_keys, stream=0, results=None, merge=False):
+    def erase(self, keys, max_key_length, key_lengths, num_keys, stream=0, results=None, merge=False,
+              remove_empty_layers=False):
+        flags = (FLAG_MERGE if merge else 0) | (FLAG_REMOVE_EMPTY_LAYERS if remove_empty_layers else 0)
         rc = self._lib.mt_erase(self._h, _ptr(keys), max_key_length, _ptr(key_lengths), num_keys, _ptr(results),
-                                FLAG_MERGE if merge else 0, _stream(stream))
+                                flags, _stream(stream))
         self._check(rc, "mt_erase")
 
     def scan(self, lower_keys, lower_key_lengths, max_key_length, max_count_per_query, num_queries,
@@ -147,9 +150,9 @@ class GpuMasstree:
 
     def mixed_batch(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
                     value_lengths, results, num_requests, stream=0, single_pass=False, bucket_keys=False,
-                    merge=False):
+                    merge=False, remove_empty_layers=False):
         flags = ((FLAG_SINGLE_PASS if single_pass else 0) | (FLAG_BUCKET_KEYS if bucket_keys else 0) |
-                 (FLAG_MERGE if merge else 0))
+                 (FLAG_MERGE if merge else 0) | (FLAG_REMOVE_EMPTY_LAYERS if remove_empty_layers else 0))
         rc = self._lib.mt_mixed_batch(self._h, _ptr(request_types), _ptr(keys), max_key_length, _ptr(key_lengths),
                                       _ptr(values), max_value_length, _ptr(value_lengths), _ptr(results),
                                       num_requests, flags, _stream(stream))

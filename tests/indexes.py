@@ -128,12 +128,13 @@ class GpuIndex(_TorchIndex):
         self.t.sync()
         return self.h(res).astype(np.uint8)
 
-    def erase(self, keys, klens, n=None, merge=False):
+    def erase(self, keys, klens, n=None, merge=False, remove_empty_layers=False):
         torch = self.torch
         keys = _u32(keys)
         n = len(keys) if n is None else n
         res = self.zeros(n, torch.bool)
-        self.t.erase(self.d(keys), keys.shape[1], self.d(_u32(klens)), n, results=res, merge=merge)
+        self.t.erase(self.d(keys), keys.shape[1], self.d(_u32(klens)), n, results=res, merge=merge,
+                     remove_empty_layers=remove_empty_layers)
         self.t.sync()
         return self.h(res).astype(np.uint8)
 
@@ -147,7 +148,8 @@ class GpuIndex(_TorchIndex):
         self.t.sync()
         return self.h(vals), self.h(vlens)
 
-    def mixed(self, types, keys, klens, vals, vlens, n=None, bucket_keys=False, merge=False):
+    def mixed(self, types, keys, klens, vals, vlens, n=None, bucket_keys=False, merge=False,
+              remove_empty_layers=False):
         torch = self.torch
         keys = _u32(keys)
         n = len(keys) if n is None else n
@@ -155,7 +157,8 @@ class GpuIndex(_TorchIndex):
         dvl = self.d(_u32(vlens))
         res = self.zeros(n, torch.bool)
         self.t.mixed_batch(self.d(np.ascontiguousarray(types, np.uint8)), self.d(keys), keys.shape[1],
-                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n, bucket_keys=bucket_keys, merge=merge)
+                           self.d(_u32(klens)), dv, dv.shape[1], dvl, res, n, bucket_keys=bucket_keys, merge=merge,
+                           remove_empty_layers=remove_empty_layers)
         self.t.sync()
         return self.h(dv), self.h(dvl), self.h(res).astype(np.uint8)
 

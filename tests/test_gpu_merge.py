@@ -105,3 +105,101 @@ def test_merge_in_mixed_batches_c2():
         same_state(g, o, c2.maxK, c2.maxV)
     finally:
         g.close()
+
+
+def _layered_keys(n_first, seed):
+    """Keys of 2-4 slices under n_first distinct first slices A: [A,B], [A,B,C]
+    and [A,B,C,D] for B in 3 values, C in 4, D in 2, so every A owns 16 trie
+    layers of one border node each (its layer 1, three layers 2, twelve
+    layers 3).  Values of 1-8 random slices."""
+    rng = np.random.default_rng(seed)
+    firsts = np.unique(rng.integers(0, 1 << 32, 2 * n_first, dtype=np.uint64).astype(np.uint32))[:n_first]
+    rng.shuffle(firsts)
+    rows = []
+    for b in (5, 9, 1 << 31):
+        rows.append([b, 0, 0, 2])
+        for c in (0, 7, 1000, 0xFFFFFFFF):
+            rows.append([b, c, 0, 3])
+            for d in (3, 4):
+                rows.append([b, c, d, 4])
+    per = np.array(rows, dtype=np.uint32)  # 39 key shapes per first slice
+    n = n_first * len(per)
+    keys = np.zeros((n, 4), np.uint32)
+    keys[:, 0] = np.repeat(firsts, len(per))
+    keys[:, 1:] = np.tile(per[:, :3], (n_first, 1))
+    lens = np.tile(per[:, 3], n_first).astype(np.uint32)
+    keys[lens < 3, 2] = 0
+    keys[lens < 4, 3] = 0
+    vlens = rng.integers(1, 9, n).astype(np.uint32)
+    vals = rng.integers(0, 1 << 32, (n, 8), dtype=np.uint64).astype(np.uint32)
+    vals[np.arange(8)[None, :] >= vlens[:, None]] = 0
+    return firsts, keys, lens, vals, vlens
+
+
+def test_remove_emptied_layers():
+    """MT_FLAG_REMOVE_EMPTY_LAYERS (the reference's erase merge level 4): every
+    key under half the first slices erased, half through mt_erase and half in a
+    mixed batch beside finds, plus every key under one second slice of other
+    first slices.  Results and contents equal the oracle's and the tree
+    validates; it holds at least 16 slabs fewer per emptied first slice than a
+    tree erased with merges alone; the erased keys go back in; erasing
+    everything then leaves only layer 0's nodes."""
+    n_first = 1000
+    firsts, keys, lens, vals, vlens = _layered_keys(n_first, 21)
+    n = len(keys)
+    gr, g0, o = GpuIndex(tile_size=8, pool_bytes=256 << 20), GpuIndex(tile_size=8, pool_bytes=256 << 20), OracleIndex()
+    try:
+        for g in (gr, g0, o):
+            g.insert(keys, lens, vals, vlens)
+        rng = np.random.default_rng(22)
+        whole = np.isin(keys[:, 0], firsts[:500])
+        part = np.isin(keys[:, 0], firsts[500:750]) & (keys[:, 1] == 9)
+        gone = np.flatnonzero(whole | part)
+        rng.shuffle(gone)
+        a, b = gone[: len(gone) // 2], gone[len(gone) // 2:]
+        ro = o.erase(keys[a], lens[a])
+        np.testing.assert_array_equal(gr.erase(keys[a], lens[a], merge=True, remove_empty_layers=True), ro)
+        np.testing.assert_array_equal(g0.erase(keys[a], lens[a], merge=True), ro)
+        keep = rng.choice(np.flatnonzero(~(whole | part)), 5000, replace=False)
+        idx = np.concatenate([b, keep])
+        types = np.concatenate([np.full(len(b), wl.REQ_ERASE, np.uint8), np.full(len(keep), wl.REQ_FIND, np.uint8)])
+        perm = rng.permutation(len(idx))
+        idx, types = idx[perm], types[perm]
+        vl = np.where(types == wl.REQ_FIND, 0, vlens[idx]).astype(np.uint32)
+        ov, ol, orr = o.mixed(types, keys[idx], lens[idx], vals[idx], vl)
+        gv, gl, grr = gr.mixed(types, keys[idx], lens[idx], vals[idx], vl, merge=True, remove_empty_layers=True)
+        _, _, g0r = g0.mixed(types, keys[idx], lens[idx], vals[idx], vl, merge=True)
+        nf = types != wl.REQ_FIND
+        np.testing.assert_array_equal(grr[nf], orr[nf])
+        np.testing.assert_array_equal(g0r[nf], orr[nf])
+        assert_found(gv[~nf], gl[~nf], ov[~nf], ol[~nf], "finds beside the erases")
+        for g in (gr, g0):
+            ok, nkeys, report = g.t.validate()
+            assert ok, report
+            assert nkeys == n - len(gone)
+        same_state(gr, o, 4, 8)
+        # 16 layers per emptied first slice, 5 (one layer 2, four layers 3) per
+        # emptied second slice.
+        assert _used(gr) <= _used(g0) - (500 * 16 + 250 * 5), (_used(gr), _used(g0))
+        # The erased keys back in: their layers are built again.
+        np.testing.assert_array_equal(gr.insert(keys[gone], lens[gone], vals[gone], vlens[gone]),
+                                      o.insert(keys[gone], lens[gone], vals[gone], vlens[gone]))
+        ok, nkeys, report = gr.t.validate()
+        assert ok, report
+        assert nkeys == n
+        same_state(gr, o, 4, 8)
+        gv, gl = gr.find(keys, lens, 8)
+        ov, ol = o.find(keys, lens, 8)
+        assert_found(gv, gl, ov, ol, "finds after the keys went back in")
+        # Everything erased: no layer below layer 0 is left.
+        full = _used(gr)
+        np.testing.assert_array_equal(gr.erase(keys, lens, merge=True, remove_empty_layers=True),
+                                      o.erase(keys, lens))
+        ok, nkeys, report = gr.t.validate()
+        assert ok, report
+        assert nkeys == 0
+        assert _used(gr) < 400, (_used(gr), full)
+        same_state(gr, o, 4, 8)
+    finally:
+        gr.close()
+        g0.close()
