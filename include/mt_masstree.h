@@ -130,7 +130,11 @@ int mt_update(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, 
               const uint32_t* values, uint32_t max_value_length, const uint32_t* value_lengths,
               uint32_t num_keys, bool* results, uint32_t flags, void* stream);
 
-/* Reference gpu_masstree::erase (gpu_masstree.hpp:132-145). */
+/* Reference gpu_masstree::erase (gpu_masstree.hpp:132-145).  flags may hold
+ * MT_FLAG_MERGE and MT_FLAG_REMOVE_EMPTY_LAYERS (as may mt_mixed_batch's): they
+ * change only the space the tree holds afterwards.  The first call with each
+ * allocates that flag's log on the device (about 32 MB and 16 MB, kept by the
+ * tree); when it does not fit, the call erases without that pass. */
 int mt_erase(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
              uint32_t num_keys, bool* results, uint32_t flags, void* stream);
 
