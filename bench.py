@@ -62,7 +62,10 @@ def parse():
                     help="extra measurements at N=1: batched (256 sub-batches, tuned persistent launch from a "
                          "CUDA graph, against one call per sub-batch), served (request loop over 64M keys, "
                          "latency against offered load, against one call per request), c1 (plain insert and "
-                         "find, 1M keys), c3 (range scan, 32M keys); 'none' to skip")
+                         "find, 1M keys), c3 (range scan, 32M keys); 'none' to skip; also space (slabs "
+                         "held after erase rounds without merges, with merges, and with merges and emptied-"
+                         "layer removal; not in the default list)")
+    ap.add_argument("--space-keys", type=int, default=1 << 21, help="tree size for the space section")
     ap.add_argument("--subbatches", type=int, default=256)
     ap.add_argument("--tune-subbatches", type=int, default=16, help="sub-batches per autotuner trial")
     ap.add_argument("--serve-keys", type=int, default=1 << 26, help="tree size for the served section")
@@ -335,6 +338,8 @@ def run_ours(args, rank, world, dist):
             extra["c1"] = run_c1(args, stream, peak_c)
         if "c3" in wanted:
             extra["c3"] = run_c3(args, stream, peak_c)
+    if world == 1 and "space" in wanted:
+        extra["space"] = run_space(args, stream)
 
     # Reduce over ranks: max time.
     if dist:
@@ -587,6 +592,46 @@ def run_c1(args, stream, peak):
             "find_roofline": {"achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(ach / peak, 4), "algorithmic_bytes": fb,
                               "note": "the 1M-key index (~150 MB of slabs) is mostly L2-resident"}}
+
+
+def run_space(args, stream):
+    """Space held after erases: a tree of C2 keys erased in four rounds of a
+    quarter of its keys each (random order), once per erase mode (no merges,
+    MT_FLAG_MERGE, MT_FLAG_MERGE | MT_FLAG_REMOVE_EMPTY_LAYERS).  Reports used
+    slabs after the preload and after every round, and each round's erase rate."""
+    import torch
+    from indexingpu_b200 import GpuMasstree
+    n = args.space_keys
+    c2 = wl.C2(n_preload=n)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    hk, hl, hv, hvl = wl.keys_threaded(c2, np.arange(n))
+    k, l, v, vl = dev(hk), dev(hl), dev(hv), dev(hvl)
+    order = np.random.default_rng(0x5BACE).permutation(n)
+    rounds = [order[i * n // 4:(i + 1) * n // 4] for i in range(4)]
+    rk = [(dev(hk[r]), dev(hl[r])) for r in rounds]
+    res = torch.zeros(n // 4 + 1, dtype=torch.bool, device="cuda")
+    modes = {"none": {}, "merge": {"merge": True}, "merge_remove_layers": {"merge": True, "remove_empty_layers": True}}
+    out = {"workload": f"{n} C2 keys (2-16 slices, 4096 shared 4-slice prefixes), erased in 4 rounds of {n // 4}",
+           "modes": {}}
+    for name, flags in modes.items():
+        with GpuMasstree(pool_bytes=2 << 30, tile_size=args.tile) as t:
+            t.set_write_tile_size(args.write_tile)
+            t.insert(k, c2.maxK, l, v, c2.maxV, vl, n, stream=stream)
+            t.sync(stream)
+            used = [t.stats()["used_slabs"]]
+            rates = []
+            for rkeys, rlens in rk:
+                m = len(rlens)
+                ms = _timed(stream, lambda: t.erase(rkeys, c2.maxK, rlens, m, stream=stream, results=res, **flags))
+                t.sync(stream)
+                assert int(res[:m].sum()) == m, "an erase round missed keys it had inserted"
+                rates.append(round(m / ms / 1e3, 2))
+                used.append(t.stats()["used_slabs"])
+            out["modes"][name] = {"used_slabs": used, "erase_mops": rates}
+    base = out["modes"]["none"]["used_slabs"][0]
+    for m in out["modes"].values():
+        m["used_pct_of_preload"] = [round(100.0 * u / base, 2) for u in m["used_slabs"]]
+    return out
 
 
 def run_c3(args, stream, peak):
