@@ -37,7 +37,7 @@ enum {
   MT_ERR_INVALID_ARG = 4,
   MT_ERR_CUDA = 5,
   MT_ERR_RETRY_LIMIT = 6,  /* an insert restarted its descent too often */
-  MT_ERR_KEY_TOO_LONG = 7, /* scan depth beyond the scan frame capacity */
+  MT_ERR_KEY_TOO_LONG = 7, /* a scan's layer stack could not grow (device API scans without an allocator) */
   MT_ERR_BATCH_TOO_LARGE = 8 /* batch larger than mt_mixed_batch_noalloc's fixed scratch */
 };
 
@@ -110,6 +110,19 @@ int mt_set_blocks_per_sm(mt_masstree* tree, uint32_t blocks_per_sm);
  * read many independent suffix lines per query and run fastest with narrow
  * tiles (more queries in flight).  New in this library. */
 int mt_set_scan_tile_size(mt_masstree* tree, uint32_t tile_size);
+
+/* Bound of every node-lock wait: lock attempts (each followed by a backoff of
+ * 64 ns to 1 us) before the waiting request gives up and the call reports
+ * MT_ERR_LOCK_TIMEOUT (default 2^20, about one second).  The reference spins
+ * without a bound (masstree_node_subwarp.hpp:217-219).  New in this library. */
+int mt_set_lock_wait(mt_masstree* tree, uint32_t attempts);
+
+/* Fault injection for tests of the bounded lock wait: set (locked != 0) or
+ * clear the LOCK bit of tree node `slab` (slab 0 is the root of trie layer 0)
+ * from the host, as a writer that never releases its lock would leave it.
+ * Synchronous; the caller must not run other work on the tree meanwhile.
+ * New in this library. */
+int mt_inject_node_lock(mt_masstree* tree, uint32_t slab, int locked);
 
 /* Reference gpu_masstree::find (gpu_masstree.hpp:86-99). */
 int mt_find(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
@@ -243,27 +256,37 @@ typedef struct mt_serve_stats {
  * (its host API serves one batch per call). */
 int mt_serve(mt_masstree* tree, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats);
 
-/* mt_mixed_batch for callers that must not allocate device memory during the
- * call: code that runs while a CUDA graph is being captured (cudaMalloc is not
- * a stream operation and breaks the capture), request loops that must never
- * wait on the driver's allocator, and programs that give the whole device
- * budget to the slab pool.  mt_mixed_batch may cudaMalloc its partition scratch
- * when a batch is larger than any before; this variant never calls cudaMalloc,
- * cudaFree or any allocating routine.  Its scratch is one fixed array of
- * 2 MiB + 128 B in the library, present on every GPU that loads it until the
- * process exits, so num_requests is limited to 262144 (1 << 18); larger
- * batches return MT_ERR_BATCH_TOO_LARGE and launch nothing.  Same arguments,
- * results and error reporting as mt_mixed_batch.
- * The first call on a device looks up the array's device address (once per
- * device, with the tree's device current); make that first call before any
- * stream capture.  All calls on one GPU share the array: calls whose work
- * overlaps on the GPU (different streams, or different trees, without ordering
- * between them) race on it and must be serialised by the caller.
+/* mt_mixed_batch for callers that cannot allocate device memory at call time:
+ * request loops that must never wait on the driver's allocator (mt_mixed_batch,
+ * given a batch larger than any before, waits for its stream and cudaMallocs
+ * new partition scratch), and programs that hand the whole device to the slab
+ * pool or to another allocator up front, where a cudaMalloc in the middle of
+ * serving fails.  This variant never calls cudaMalloc, cudaFree or any
+ * allocating routine.  Its scratch is one fixed array of 2 MiB + 128 B in the
+ * library, present on every GPU that loads it until the process exits, so
+ * num_requests is limited to 262144 (1 << 18); larger batches return
+ * MT_ERR_BATCH_TOO_LARGE and launch nothing.  It takes the arguments of
+ * mt_mixed_batch without flags and behaves as mt_mixed_batch with flags = 0
+ * (same results and error reporting; the finds and then the writes are served
+ * as two passes on `stream`).
+ * The tree's device must be current (else MT_ERR_INVALID_ARG).  The first call
+ * on a device looks up the array's device address there (once per device);
+ * make that first call before any stream capture.  All calls on one GPU share
+ * the array and it keeps the last call's contents: calls whose work overlaps on
+ * the GPU (different streams, or different trees, without ordering between
+ * them) race on it and must be serialised by the caller.
  * No counterpart in the reference. */
 int mt_mixed_batch_noalloc(mt_masstree* tree, const uint8_t* request_types, const uint32_t* keys,
                            uint32_t max_key_length, const uint32_t* key_lengths, uint32_t* values,
                            uint32_t max_value_length, uint32_t* value_lengths, bool* results,
                            uint32_t num_requests, void* stream);
+
+/* Device view of the tree for kernels that call the device API
+ * (include/mt/device.cuh, gpu_masstree_device::from): copies the view, a
+ * plain struct of view_bytes bytes (checked), to *view.  The view stays valid
+ * until mt_destroy.  New in this library (the reference's kernels take the
+ * host object itself by value, include/gpu_masstree.hpp:194-971). */
+int mt_device_view(mt_masstree* tree, void* view, size_t view_bytes);
 
 /* Wait for `stream`, then return (and clear) the first device error recorded
  * since the previous mt_sync (MT_OK if none). */

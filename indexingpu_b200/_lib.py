@@ -19,6 +19,8 @@ SIGNATURES = {
     "mt_set_write_tile_size": (_int, [_p, _u32]),
     "mt_set_blocks_per_sm": (_int, [_p, _u32]),
     "mt_set_scan_tile_size": (_int, [_p, _u32]),
+    "mt_set_lock_wait": (_int, [_p, _u32]),
+    "mt_inject_node_lock": (_int, [_p, _u32, _int]),
     "mt_find": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _u32, _p]),
     "mt_insert": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),
     "mt_update": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),
@@ -36,6 +38,7 @@ SIGNATURES = {
     "mt_validate": (_int, [_p, ctypes.POINTER(_u64), ctypes.c_char_p, ctypes.c_size_t]),
     "mt_selftest_line_atomicity": (_int, [_u32, _u32, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "mt_serve": (_int, [_p, _p, _p, _p]),
+    "mt_device_view": (_int, [_p, _p, ctypes.c_size_t]),
 }
 
 

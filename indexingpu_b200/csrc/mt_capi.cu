@@ -104,7 +104,11 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) scan_kernel(tree
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
-  scan_frame* frames = a.frames + (size_t)tile_id * kScanDepth;
+  // Layer frames: kScanDepth per tile in the tree's scratch, deeper ones
+  // spill to slabs from the tile's cache.
+  slab_cache<T> cache;
+  cache.init(tv.pool, tile_id);
+  scan_frames<T> frames(a.frames + (size_t)tile_id * kScanDepth, kScanDepth, &cache);
   // Queries per tile and round: T on large batches, fewer on small ones so that
   // every tile gets work (as in serve_requests).
   const uint32_t per = max(1u, min((uint32_t)T, (a.n + num_tiles - 1u) / num_tiles));
@@ -136,11 +140,12 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) scan_kernel(tree
       const uint32_t* lower = a.lower + (size_t)q * a.max_key_length;
       const uint32_t* upper = a.upper ? a.upper + (size_t)q * a.max_key_length : nullptr;
       const uint32_t c = coop_scan<T, CONC>(t, tv, lower, ll, a.use_upper != 0u && upper != nullptr, upper, ul,
-                                           a.max_count, o, frames, kScanDepth);
+                                           a.max_count, o, frames);
       if (t.rank == r) cnt = c;
     }
     if (valid && a.counts) a.counts[i] = cnt;
   }
+  cache.release(t, tv.pool);
 }
 
 
@@ -438,6 +443,7 @@ int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
   p.num_slabs = (uint32_t)nslabs;
   p.num_shards = kShards;
   p.shard_slabs = shard_slabs;
+  p.lock_spins = kLockSpins;
   cudaError_t e = cudaMemset(p.ctr, 0, ctr_bytes + err_bytes);
   // Root of trie layer 0 = slab 0 (shard 0's bump pointer starts past it).
   uint32_t root_img[32] = {0};
@@ -532,6 +538,23 @@ int mt_set_scan_tile_size(mt_masstree* t, uint32_t ts) {
   if (!t || (ts != 0 && !valid_tile(ts))) return MT_ERR_INVALID_ARG;
   t->scan_tile_size = ts;
   return MT_OK;
+}
+
+int mt_set_lock_wait(mt_masstree* t, uint32_t attempts) {
+  if (!t || attempts == 0) return MT_ERR_INVALID_ARG;
+  t->tv.pool.lock_spins = attempts;
+  return MT_OK;
+}
+
+int mt_inject_node_lock(mt_masstree* t, uint32_t slab, int locked) {
+  if (!t || !t->tv.pool.valid(slab)) return MT_ERR_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return MT_ERR_CUDA;
+  uint32_t* mw = t->tv.pool.addr(slab) + WORD_META;
+  uint32_t meta = 0;
+  if (cudaMemcpy(&meta, mw, sizeof(meta), cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_CUDA;
+  // The LOCK bit is outside the node checksum, so the image stays valid.
+  meta = locked ? (meta | META_LOCK) : (meta & ~META_LOCK);
+  return cuda_status(cudaMemcpy(mw, &meta, sizeof(meta), cudaMemcpyHostToDevice));
 }
 
 int mt_set_blocks_per_sm(mt_masstree* t, uint32_t b) {
@@ -639,6 +662,17 @@ int mt_sync(mt_masstree* t, void* stream) {
   return (int)code;
 }
 
+int mt_device_view(mt_masstree* t, void* view, size_t view_bytes) {
+  if (!t || !view || view_bytes != sizeof(tree_view)) return MT_ERR_INVALID_ARG;
+  tree_view v = t->tv;
+  v.merge_log = nullptr;  // the device API never logs merges
+  v.merge_cap = 0;
+  v.layer_log = nullptr;
+  v.layer_cap = 0;
+  std::memcpy(view, &v, sizeof(v));
+  return MT_OK;
+}
+
 int mt_reclaim(mt_masstree* t, void* stream) {
   if (!t) return MT_ERR_INVALID_ARG;
   return launch_reclaim(t, (cudaStream_t)stream);
@@ -685,7 +719,7 @@ const char* mt_status_string(int s) {
     case MT_ERR_INVALID_ARG: return "invalid argument";
     case MT_ERR_CUDA: return "CUDA error";
     case MT_ERR_RETRY_LIMIT: return "retry limit reached";
-    case MT_ERR_KEY_TOO_LONG: return "key deeper than scan frame capacity";
+    case MT_ERR_KEY_TOO_LONG: return "scan layer stack could not grow";
     case MT_ERR_BATCH_TOO_LARGE: return "batch larger than the fixed no-allocation scratch";
     default: return "unknown status";
   }
@@ -886,11 +920,10 @@ extern "C" int mt_selftest_line_atomicity(uint32_t tile_size, uint32_t nlines, u
 //
 // mt_mixed_batch keeps its partition scratch in memory it allocates with
 // cudaMalloc the first time a batch is larger than any before.  Some callers
-// cannot allocate at that point: code running while a CUDA graph is being
-// captured (cudaMalloc is not a stream operation and breaks the capture),
-// latency-critical request loops that must never take the driver's allocation
-// lock, and hosts that hand the whole device budget to the slab pool up front.
-// mt_mixed_batch_noalloc serves them: its partition scratch is the fixed
+// cannot allocate at that point: latency-critical request loops that must never
+// wait for the driver's allocator, and hosts that hand the whole device budget
+// to the slab pool (or to another allocator) up front, where a late cudaMalloc
+// fails.  mt_mixed_batch_noalloc serves them: its partition scratch is the fixed
 // file-scope array below, sized for kNoAllocMaxRequests requests (2 MiB plus
 // one line, held on every GPU that loads this library until the process exits).
 
@@ -906,12 +939,11 @@ namespace {
 std::mutex g_noalloc_mu;
 uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device with that device current and kept.
-int noalloc_scratch(uint32_t** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return MT_ERR_CUDA;
+// Device address of g_noalloc_scratch on device `dev`, which must be current.
+// In host code the array's name is only a host-side stand-in, so the address
+// is looked up once per device with that device current and kept.
+int noalloc_scratch(int dev, uint32_t** out) {
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return MT_ERR_CUDA;
   std::lock_guard<std::mutex> g(g_noalloc_mu);
   if (!g_noalloc_addr[dev]) {
     void* p = nullptr;
@@ -929,8 +961,12 @@ extern "C" int mt_mixed_batch_noalloc(mt_masstree* t, const uint8_t* types, cons
   if (!t || (n && (!types || !keys || !values || !vlens || maxK == 0 || maxV == 0))) return MT_ERR_INVALID_ARG;
   if (n > kNoAllocMaxRequests) return MT_ERR_BATCH_TOO_LARGE;
   if (n == 0) return MT_OK;
+  // The scratch address belongs to the current device: it must be the tree's.
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MT_ERR_CUDA;
+  if (dev != t->device) return MT_ERR_INVALID_ARG;
   uint32_t* scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
+  int rc = noalloc_scratch(dev, &scratch);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   batch_args a{};

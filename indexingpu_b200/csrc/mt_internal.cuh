@@ -9,7 +9,7 @@ namespace mtb {
 
 constexpr int kBlock = 128;
 constexpr uint32_t kShards = 64;
-constexpr uint32_t kScanDepth = 256;  // trie layers a scan can stack
+constexpr uint32_t kScanDepth = 32;   // scan layer frames per tile in scratch (deeper ones spill to slabs)
 // In the persistent launch of mt_mixed_batches, sub-batches of at least this
 // many requests serve their classes one after the other with a grid barrier
 // between them (all warps in the same code at a time, faster on large

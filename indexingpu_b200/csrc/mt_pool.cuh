@@ -51,7 +51,7 @@ struct pool_view {
   uint32_t num_slabs;
   uint32_t num_shards;
   uint32_t shard_slabs;
-  uint32_t pad_;
+  uint32_t lock_spins;    // lock attempts before MT_ERR_LOCK_TIMEOUT (mt_set_lock_wait)
 
   MT_HD uint32_t* addr(uint32_t i) const { return slabs + (size_t)i * 32u; }
   MT_HD bool valid(uint32_t i) const { return i < num_slabs; }

@@ -27,8 +27,9 @@ struct tile {
   uint32_t base;  // first warp lane of the tile
   uint32_t mask;  // warp lane mask of the tile
 
-  MT_DEV tile() {
-    const uint32_t wl = threadIdx.x & 31u;
+  MT_DEV tile() : tile(threadIdx.x & 31u) {}  // 1-D blocks: lane = threadIdx.x % 32
+  // From the warp lane (any block shape: pass %laneid).
+  MT_DEV explicit tile(uint32_t wl) {
     rank = wl % T;
     base = wl - rank;
     mask = (T == 32) ? 0xFFFFFFFFu : (((1u << T) - 1u) << base);
@@ -45,6 +46,12 @@ struct tile {
   MT_DEV void sync() const { __syncwarp(mask); }
   MT_DEV bool leader() const { return rank == 0; }
 };
+
+MT_DEV uint32_t lane_id() {
+  uint32_t l;
+  asm("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
 
 // Memory orders for node traffic.
 //   NC      : read-only path (no writer in the same launch); texture/L1 path.

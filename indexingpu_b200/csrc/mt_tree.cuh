@@ -33,7 +33,7 @@
 namespace mtb {
 
 constexpr uint32_t kMaxHops = 1u << 16;     // node visits per operation
-constexpr uint32_t kLockSpins = 1u << 20;   // lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
+constexpr uint32_t kLockSpins = 1u << 20;   // default lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
 constexpr uint32_t kMaxRestarts = 1u << 14;
 
 #ifndef MT_CONC_LOAD
@@ -93,7 +93,7 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
   uint32_t* mw = p.addr(idx) + WORD_META;
   uint32_t backoff = 64u;
   uint32_t jitter = (idx * 0x9E3779B1u) ^ (uint32_t)clock();
-  for (uint32_t it = 0; it < kLockSpins; ++it) {
+  for (uint32_t it = 0; it < p.lock_spins; ++it) {
     uint32_t old = META_LOCK;
     if (t.leader()) {
       if (it == 0u || !(ld_relaxed_u32(mw) & META_LOCK)) old = atom_or_acquire(mw, META_LOCK);
@@ -101,8 +101,8 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
     old = t.shfl(old, 0);
     if (!(old & META_LOCK)) {
       t.sync();
-      // No writer can publish this node while we hold its lock; a checksum
-      // mismatch here would be a bug, reported as corruption.
+      // The previous holder's image may still be landing (its publishing
+      // store also released the lock): reload until the checksum matches.
       return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
@@ -123,12 +123,19 @@ MT_DEV void publish_locked(const tile<T>& t, const pool_view& p, node<T>& nd) {
   nd.template store<st_order::RELEASE>(t, p);
 }
 
-// Publish the node image, then release its lock.
+// Publish the node image and release its lock with the same line store (the
+// stored meta word has LOCK clear): one release store instead of a store and
+// a release atomic.  The next locker reloads the node after its lock atomic
+// and accepts only an image whose checksum (which covers the version) matches,
+// so it never works on a mix of this image and the one before; each of its
+// lanes then stores the words it loaded, after the values it read
+// (per-location coherence), so no word of this image is lost.
 template <int T>
 MT_DEV void publish_unlock(const tile<T>& t, const pool_view& p, node<T>& nd) {
-  publish_locked(t, p, nd);
-  unlock_node(t, p, nd.idx);
-  nd.meta &= ~META_LOCK;
+  nd.meta = (nd.meta & ~META_LOCK) + META_VERSION_ONE;
+  nd.encode_header(t);
+  nd.seal(t);
+  nd.template store<st_order::RELEASE>(t, p);
 }
 
 // Write a node that no other tile can reach yet.
@@ -728,14 +735,117 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
 
 // ---- scan ----------------------------------------------------------------------------
 
-// Per-layer scan frame kept in global scratch: border node holding the LINK we
-// descended through, the LINK's slice, and whether the layer was on the upper
-// bound's path.
+// Per-layer scan frame: border node holding the LINK we descended through,
+// the LINK's slice, and whether the layer was on the upper bound's path.
 struct scan_frame {
   uint32_t node;
   uint32_t slice;
   uint32_t upper_tight;
   uint32_t pad;
+};
+
+// The layer stack of one scan (the reference's tile-local dynamic_stack, which
+// keeps 31 entries in registers and spills to slabs, include/dynamic_stack.hpp:
+// 30-152).  Frames [0, fast_cap) live in a caller-provided global array; deeper
+// frames spill to pool slabs of kFramesPerSlab frames each (frame k at words
+// 4k..4k+3, word 31 = the slab below), taken from the tile's slab cache and
+// retired when the stack shrinks or the scan ends.  Spill slabs are private to
+// the tile.  Without a cache (and for fast_cap layers and more) a deeper scan
+// reports MT_ERR_KEY_TOO_LONG.  Every member function is called by the whole
+// tile; slice_at is per lane.
+constexpr uint32_t kFramesPerSlab = 7;
+
+template <int T>
+struct scan_frames {
+  scan_frame* fast = nullptr;
+  uint32_t fast_cap = 0;
+  slab_cache<T>* cache = nullptr;
+  uint32_t cur = kInvalid;  // top spill slab (uniform)
+  uint32_t base = 0;        // first spilled frame index (above fast_cap) held by `cur`
+
+  MT_DEV scan_frames(scan_frame* f, uint32_t cap, slab_cache<T>* c) : fast(f), fast_cap(cap), cache(c) {}
+
+  // Drop spill slabs until `cur` holds spilled frame i (or none are left).
+  MT_DEV void shrink_to(const tile<T>& t, const pool_view& p, uint32_t i) {
+    while (cur != kInvalid && i < base) {
+      const uint32_t below = ld_word<ld_order::RELAXED>(p.addr(cur) + 31);
+      t.sync();
+      if (t.leader()) retire_slab(p, cur);
+      cur = below;
+      base = base >= kFramesPerSlab ? base - kFramesPerSlab : 0u;
+    }
+  }
+  MT_DEV bool push(const tile<T>& t, const pool_view& p, uint32_t layer, const scan_frame& f) {
+    if (layer < fast_cap) {
+      if (t.leader()) fast[layer] = f;
+      t.sync();
+      return true;
+    }
+    const uint32_t i = layer - fast_cap;
+    shrink_to(t, p, i);
+    if (cur == kInvalid || i >= base + kFramesPerSlab) {
+      if (cache == nullptr) {
+        if (t.leader()) record_error(p, ERR_KEY_TOO_LONG);
+        return false;
+      }
+      const uint32_t s = cache->allocate(t, p);
+      if (s == kInvalid) return false;
+      if (t.leader()) p.addr(s)[31] = cur;
+      base = (cur == kInvalid) ? 0u : base + kFramesPerSlab;
+      cur = s;
+    }
+    if (t.leader()) {
+      uint32_t* w = p.addr(cur) + 4u * (i - base);
+      w[0] = f.node;
+      w[1] = f.slice;
+      w[2] = f.upper_tight;
+      w[3] = f.pad;
+    }
+    t.sync();
+    return true;
+  }
+  // Frame `layer` after the stack shrank to it (frames above it are dropped).
+  MT_DEV scan_frame pop_to(const tile<T>& t, const pool_view& p, uint32_t layer) {
+    if (layer < fast_cap) {
+      if (cur != kInvalid) release(t, p);
+      return fast[layer];
+    }
+    const uint32_t i = layer - fast_cap;
+    shrink_to(t, p, i);
+    const uint32_t* w = p.addr(cur) + 4u * (i - base);
+    scan_frame f;
+    f.node = w[0];
+    f.slice = w[1];
+    f.upper_tight = w[2];
+    f.pad = w[3];
+    return f;
+  }
+  // LINK slice of frame i below the top of the stack (per lane).
+  MT_DEV uint32_t slice_at(const pool_view& p, uint32_t i) const {
+    if (i < fast_cap) return fast[i].slice;
+    const uint32_t j = i - fast_cap;
+    uint32_t s = cur, b = base;
+    while (j < b && s != kInvalid) {
+      s = p.addr(s)[31];
+      b -= kFramesPerSlab;
+    }
+    return s == kInvalid ? 0u : p.addr(s)[4u * (j - b) + 1u];
+  }
+  // Retire every spill slab (the scan ended).
+  MT_DEV void release(const tile<T>& t, const pool_view& p) {
+    t.sync();
+    if (t.leader()) {
+      uint32_t c = cur;
+      while (c != kInvalid) {
+        const uint32_t below = p.addr(c)[31];
+        retire_slab(p, c);
+        c = below;
+      }
+    }
+    cur = kInvalid;
+    base = 0;
+    t.sync();
+  }
 };
 
 struct scan_out {
@@ -749,7 +859,7 @@ struct scan_out {
 
 // Emit one result: key = frames[0..layer) slices ++ slice ++ suffix rest.
 template <int T, ld_order OS>
-MT_DEV void scan_emit(const tile<T>& t, const pool_view& p, const scan_frame* frames, uint32_t layer,
+MT_DEV void scan_emit(const tile<T>& t, const pool_view& p, const scan_frames<T>& frames, uint32_t layer,
                       uint32_t slice, uint32_t state, uint32_t v, const suffix_head<T>* h,
                       const scan_out& o, uint32_t c) {
   uint32_t rest = 0, vlen = 1;
@@ -757,7 +867,7 @@ MT_DEV void scan_emit(const tile<T>& t, const pool_view& p, const scan_frame* fr
   const uint32_t klen = layer + 1u + rest;
   if (o.keys) {
     uint32_t* row = o.keys + (size_t)c * o.maxK;
-    for (uint32_t i = t.rank; i < layer && i < o.maxK; i += T) row[i] = frames[i].slice;
+    for (uint32_t i = t.rank; i < layer && i < o.maxK; i += T) row[i] = frames.slice_at(p, i);
     if (t.leader() && layer < o.maxK) row[layer] = slice;
     if (rest) {
       // Key rest: data slices [0, rest) of the chain.
@@ -784,12 +894,27 @@ MT_DEV void scan_emit(const tile<T>& t, const pool_view& p, const scan_frame* fr
 }
 
 // Ordered scan from `lower` (inclusive) for at most max_count keys, stopping
-// after `upper` (inclusive) when use_upper.  frames: scratch of frame_cap frames
-// for this tile.  Returns the number of keys written.
+// after `upper` (inclusive) when use_upper.  frames: the tile's layer stack
+// (empty on entry; emptied again on return).  Returns the number of keys
+// written.
+template <int T, bool CONCURRENT>
+MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint32_t* lower, uint32_t llen,
+                               bool use_upper, const uint32_t* upper, uint32_t ulen, uint32_t max_count,
+                               const scan_out& o, scan_frames<T>& frames);
+
 template <int T, bool CONCURRENT>
 MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t* lower, uint32_t llen,
                           bool use_upper, const uint32_t* upper, uint32_t ulen, uint32_t max_count,
-                          const scan_out& o, scan_frame* frames, uint32_t frame_cap) {
+                          const scan_out& o, scan_frames<T>& frames) {
+  const uint32_t c = coop_scan_walk<T, CONCURRENT>(t, tv, lower, llen, use_upper, upper, ulen, max_count, o, frames);
+  if (frames.cur != kInvalid) frames.release(t, tv.pool);
+  return c;
+}
+
+template <int T, bool CONCURRENT>
+MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint32_t* lower, uint32_t llen,
+                               bool use_upper, const uint32_t* upper, uint32_t ulen, uint32_t max_count,
+                               const scan_out& o, scan_frames<T>& frames) {
   constexpr ld_order O = CONCURRENT ? kConc : ld_order::NC;
   constexpr ld_order OS = CONCURRENT ? kConcSuffix : ld_order::NC;
   const pool_view& p = tv.pool;
@@ -850,16 +975,12 @@ MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t*
         }
       }
       if (st == KS_LINK) {
-        if (layer + 1u >= frame_cap) { if (t.leader()) record_error(p, ERR_KEY_TOO_LONG); return count; }
-        if (t.leader()) {
-          scan_frame f;
-          f.node = nd.idx;
-          f.slice = s;
-          f.upper_tight = utight ? 1u : 0u;
-          f.pad = 0u;
-          frames[layer] = f;
-        }
-        t.sync();
+        scan_frame f;
+        f.node = nd.idx;
+        f.slice = s;
+        f.upper_tight = utight ? 1u : 0u;
+        f.pad = 0u;
+        if (!frames.push(t, p, layer, f)) return count;
         ++layer;
         ltight = child_ltight;
         utight = child_utight;
@@ -889,7 +1010,7 @@ MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t*
     if (layer == 0u) return count;
     t.sync();
     --layer;
-    const scan_frame f = frames[layer];
+    const scan_frame f = frames.pop_to(t, p, layer);
     utight = f.upper_tight != 0u;
     if (utight && f.slice == upper[layer]) return count;  // the LINK was upper's own path
     if (f.slice == 0xFFFFFFFFu) {

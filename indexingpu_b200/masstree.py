@@ -106,6 +106,14 @@ class GpuMasstree:
     def set_blocks_per_sm(self, blocks_per_sm):
         self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
 
+    def set_lock_wait(self, attempts):
+        """Lock attempts before a waiting request reports MT_ERR_LOCK_TIMEOUT."""
+        self._check(self._lib.mt_set_lock_wait(self._h, attempts), "mt_set_lock_wait")
+
+    def inject_node_lock(self, slab, locked=True):
+        """Test hook: set or clear the LOCK bit of node `slab` from the host."""
+        self._check(self._lib.mt_inject_node_lock(self._h, slab, 1 if locked else 0), "mt_inject_node_lock")
+
     # -- host API (reference gpu_masstree.hpp:86-191) ----------------------------
     def find(self, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, num_keys,
              stream=0, concurrent=False):

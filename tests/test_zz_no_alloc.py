@@ -1,6 +1,7 @@
 """mt_mixed_batch_noalloc: the mixed batch for callers that cannot allocate
-device memory during the call (stream capture, allocation-free request loops,
-programs that give the whole device to the slab pool).  It must give exactly
+device memory during the call (request loops that must never wait for the
+driver's allocator, programs that give the whole device to the slab pool or to
+another allocator up front).  It must give exactly
 the results of mt_mixed_batch: two identical trees, two mixed batches in a row,
 one tree driven through each entry point, compared request by request and by
 final contents.  Collected last so a failure here leaves every other test run.
