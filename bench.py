@@ -393,6 +393,10 @@ def run_ours(args, rank, world, dist):
             "pool": {"used_slabs": stats["used_slabs"], "total_slabs": stats["total_slabs"]},
         }
         res.update(extra)
+        if "served" in res:
+            # Served peaks against this run's plain 1M-request mixed batches.
+            for k in ("served_peak", "online_peak"):
+                res["served"][k + "_over_plain_1M_batch"] = round(res["served"][k]["mops"] / value, 3)
     return res
 
 
@@ -508,13 +512,20 @@ def run_served(args, tree, c2, stream):
     fresh0 = args.serve_keys + (1 << 31)
     n = args.serve_requests
 
-    def once(i, rate, plain=False, n_req=n):
+    def once(i, rate, plain=False, n_req=n, online=False):
         st = wl.serve_stream(c5, n_req, rate_per_s=rate, min_ops=1, max_ops=4096, seed=0xC5 + i,
                              first_fresh=fresh0 + i * (1 << 24))
-        dev = _dev_ops(torch, st)
+        if online:
+            # Host (pinned) buffers: each request is uploaded when it is
+            # submitted and its results downloaded when it completes.
+            dev = {k: torch.from_numpy(np.ascontiguousarray(st[k])).pin_memory()
+                   for k in ("types", "keys", "lens", "vals", "vlens")}
+            dev["res"] = torch.zeros(len(st["types"]), dtype=torch.bool).pin_memory()
+        else:
+            dev = _dev_ops(torch, st)
         lat, stats = tree.serve(dev["types"], dev["keys"], MAXK, dev["lens"], dev["vals"], MAXV, dev["vlens"],
                                 dev["res"], st["first"], st["nops"], st["arrival_ns"], plain=plain,
-                                chunk_ops=args.serve_chunk)
+                                chunk_ops=args.serve_chunk, online=online)
         tree.sync(stream)
         ops = int(st["nops"].sum())
         p = np.percentile(lat / 1e3, [50, 99, 99.9])
@@ -529,6 +540,14 @@ def run_served(args, tree, c2, stream):
         r = once(1 + j, frac * peak["req_s"])
         r["load"] = frac
         curve.append(r)
+    # The same through the online server API from host buffers (uploads and
+    # downloads inside every request's latency).
+    online_peak = once(20, None, online=True)
+    online_curve = []
+    for j, frac in enumerate((0.1, 0.25, 0.5, 0.75, 0.9, 1.0)):
+        r = once(21 + j, frac * online_peak["req_s"], online=True)
+        r["load"] = frac
+        online_curve.append(r)
     n_plain = max(200, n // 4)
     plain_peak = once(10, None, plain=True, n_req=n_plain)
     rate_eq = 0.5 * plain_peak["req_s"]
@@ -538,6 +557,9 @@ def run_served(args, tree, c2, stream):
                         "Poisson arrivals (seed 0xC5+i); latency = arrival to completion seen by the host",
             "tree_keys": args.serve_keys, "grow_s": round(t_grow, 1), "chunk_ops": args.serve_chunk,
             "served_peak": peak, "served_curve": curve,
+            "online_note": "mt_server_* from pinned host buffers: upload, device work and download of each "
+                           "request inside its latency",
+            "online_peak": online_peak, "online_curve": online_curve,
             "plain_per_request_peak": plain_peak, "plain_at_half_its_peak": plain_half,
             "served_at_same_load": served_half,
             "served_over_plain_mops": round(peak["mops"] / plain_peak["mops"], 2)}

@@ -87,6 +87,9 @@ typedef struct mt_stats_t {
   uint32_t tile_size;
   uint32_t device_error;    /* first device error since the last mt_sync */
   uint32_t device_error_count;
+  uint32_t device_error_site; /* where that error (or, if none is pending, the one the last mt_sync
+                                 returned) was detected: source file number << 16 | line (diagnostics) */
+  uint32_t reserved;
 } mt_stats_t;
 
 /* Construction.  Replaces gpu_masstree(allocator(pool_ratio), reclaimer())
@@ -214,6 +217,9 @@ int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t 
 /* Serving (mt_serve). */
 #define MT_SERVE_SERVED 0u /* device-resident request loop with continuous admission */
 #define MT_SERVE_PLAIN 1u  /* one synchronous mt_mixed_batch call per request, in arrival order */
+#define MT_SERVE_ONLINE 2u /* the plan's op buffers are HOST memory: each request is submitted at its
+                              arrival time through mt_server_submit (its upload and the download of
+                              its results are part of its latency) and polled to completion */
 
 typedef struct mt_serve_plan {
   /* Ops of every request, concatenated (device pointers; request r owns ops
@@ -232,7 +238,7 @@ typedef struct mt_serve_plan {
   const uint32_t* request_num_ops;
   const uint64_t* arrival_ns;  /* arrival time after the start of the run */
   uint32_t num_requests;
-  uint32_t mode;               /* MT_SERVE_SERVED or MT_SERVE_PLAIN */
+  uint32_t mode;               /* MT_SERVE_SERVED, MT_SERVE_PLAIN or MT_SERVE_ONLINE */
   uint32_t chunk_ops;          /* ops per device work item (0 = chosen per request from the backlog) */
   uint32_t epoch_us;           /* device time per launch of the serving loop (0 = 20000) */
   float memory_budget;         /* admit while slabs in use stay under this share of the pool (0 = 0.9) */
@@ -255,6 +261,50 @@ typedef struct mt_serve_stats {
  * requests of one reference mixed_batch.  No counterpart in the reference
  * (its host API serves one batch per call). */
 int mt_serve(mt_masstree* tree, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats);
+
+/* Online serving (mt_server_*): a device-resident request loop that clients
+ * feed with requests from host memory while it runs.  mt_server_submit takes
+ * one request (num_ops ops of any kind, the buffers of one mt_mixed_batch call,
+ * in HOST memory, pinned for the copies to overlap) and returns at once with a
+ * ticket; a host thread of the server admits queued requests in submission
+ * order while the staging space and the memory budget allow, uploads their ops
+ * (the upload is part of the request's latency), publishes them as work items
+ * to the device loop (the persistent kernel of mt_serve), downloads each
+ * request's results into its host buffers when the device completes it, and
+ * then marks the ticket done.  Requests in flight together have no order among
+ * each other, as the requests of one mixed batch; a request's buffers must stay
+ * untouched until mt_server_poll reports it done.  Submit and poll may be
+ * called from any host thread; while a server runs, nothing else may be called
+ * on its tree.  No counterpart in the reference (its host API serves one batch
+ * per call, gpu_masstree.hpp:173-191). */
+typedef struct mt_server mt_server;
+
+typedef struct mt_server_config {
+  uint32_t max_key_length;
+  uint32_t max_value_length;
+  uint32_t max_ops_in_flight;      /* device staging for admitted ops (0 = 1 << 20) */
+  uint32_t max_requests_in_flight; /* admitted and not yet done (0 = 65536) */
+  uint32_t chunk_ops;              /* ops per device work item (0 = chosen per request from the backlog) */
+  uint32_t epoch_us;               /* device time per launch of the loop (0 = 20000) */
+  float memory_budget;             /* admit while slabs in use stay under this share of the pool (0 = 0.9) */
+  uint32_t reserved;
+} mt_server_config;
+
+/* Start serving `tree` (allocates the staging and starts the host thread and
+ * the device loop). */
+int mt_server_start(mt_masstree* tree, const mt_server_config* config, mt_server** out);
+/* Queue one request of num_ops ops (1 .. max_ops_in_flight); *ticket receives
+ * its ticket.  key_lengths and results may be NULL, as for mt_mixed_batch. */
+int mt_server_submit(mt_server* server, const uint8_t* request_types, const uint32_t* keys,
+                     const uint32_t* key_lengths, uint32_t* values, uint32_t* value_lengths, bool* results,
+                     uint32_t num_ops, uint64_t* ticket);
+/* *done = 1 once the request's results are in its host buffers (then
+ * *latency_ns, if not NULL, receives the time from submit to done), else 0. */
+int mt_server_poll(mt_server* server, uint64_t ticket, int* done, uint64_t* latency_ns);
+/* Serve every submitted request, stop the loop and free the server (the tree
+ * stays).  Returns the first device error of the run (as mt_sync), or
+ * MT_ERR_LOCK_TIMEOUT if the queued work did not drain within 60 s. */
+int mt_server_stop(mt_server* server);
 
 /* mt_mixed_batch for callers that cannot allocate device memory at call time:
  * request loops that must never wait on the driver's allocator (mt_mixed_batch,

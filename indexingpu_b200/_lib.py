@@ -39,6 +39,10 @@ SIGNATURES = {
     "mt_selftest_line_atomicity": (_int, [_u32, _u32, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "mt_serve": (_int, [_p, _p, _p, _p]),
     "mt_device_view": (_int, [_p, _p, ctypes.c_size_t]),
+    "mt_server_start": (_int, [_p, _p, ctypes.POINTER(_p)]),
+    "mt_server_submit": (_int, [_p, _p, _p, _p, _p, _p, _p, _u32, ctypes.POINTER(_u64)]),
+    "mt_server_poll": (_int, [_p, _u64, ctypes.POINTER(_int), ctypes.POINTER(_u64)]),
+    "mt_server_stop": (_int, [_p]),
 }
 
 
@@ -52,6 +56,8 @@ class MtStats(ctypes.Structure):
         ("tile_size", _u32),
         ("device_error", _u32),
         ("device_error_count", _u32),
+        ("device_error_site", _u32),
+        ("reserved", _u32),
     ]
 
 
@@ -70,6 +76,19 @@ class MtServePlan(ctypes.Structure):
         ("arrival_ns", _p),
         ("num_requests", _u32),
         ("mode", _u32),
+        ("chunk_ops", _u32),
+        ("epoch_us", _u32),
+        ("memory_budget", ctypes.c_float),
+        ("reserved", _u32),
+    ]
+
+
+class MtServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("max_key_length", _u32),
+        ("max_value_length", _u32),
+        ("max_ops_in_flight", _u32),
+        ("max_requests_in_flight", _u32),
         ("chunk_ops", _u32),
         ("epoch_us", _u32),
         ("memory_budget", ctypes.c_float),

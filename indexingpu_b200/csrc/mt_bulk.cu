@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) bulk_node_kernel
     node<32> nd;
     nd.idx = ids[k];
     if (!p.valid(nd.idx)) {
-      if (t.leader()) record_error(p, ERR_OOM);
+      if (t.leader()) record_error(p, ERR_OOM, MT_AT(SRC_BULK));
       continue;
     }
     const uint32_t g = t.rank;  // one word per lane
@@ -337,7 +337,7 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
   // Decline when one bucket is large, or the keys crowd into few buckets
   // (first slices shared by many keys: little to build, and the in-bucket
   // sort would be slow), or fewer than half the keys are valid.
-  bool declined = !rc && (h[1] > 2048u || h[4] < m / 64u || m < n / 2u);
+  bool declined = !rc && (h[1] > 2048u || h[4] < std::min<uint32_t>(m, kBuckets) / 64u || m < n / 2u);
   if (!rc && !declined) {
     bulk_scan_kernel<<<1, 1024, 0, s>>>(b);
     bulk_scatter_kernel<<<grid, 256, 0, s>>>(b);

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) scan_kernel(tree
       ulen = a.upper_lengths ? a.upper_lengths[i] : a.max_key_length;
     }
     const bool bad = valid && (llen > a.max_key_length || (a.use_upper && ulen > a.max_key_length));
-    if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
+    if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG, MT_AT(SRC_CAPI));
     const uint32_t nreq = min(per, a.n - base);
     for (uint32_t r = 0; r < nreq; ++r) {
       if (t.shfl((uint32_t)bad, (int)r)) continue;
@@ -197,7 +197,7 @@ __global__ void reclaim_kernel(pool_view p) {
       top = max(*p.top(s), 0);
       n = *p.limbo_count(s);
       if (top + n > (int)p.shard_slabs) {
-        record_error(p, ERR_CORRUPT);
+        record_error(p, ERR_CORRUPT, MT_AT(SRC_CAPI));
         n = 0;
       }
     }
@@ -300,8 +300,7 @@ int launch_reclaim(mt_masstree* t, cudaStream_t s) {
 template <int T, int OP, bool CONC>
 int launch_batch_t(mt_masstree* t, const batch_args& a, cudaStream_t s) {
   const void* fn = (const void*)batch_kernel<T, OP, CONC>;
-  const int grid = grid_for(t, fn);
-  batch_kernel<T, OP, CONC><<<grid, kBlock, 0, s>>>(t->tv, a);
+  batch_kernel<T, OP, CONC><<<grid_for(t, fn), kBlock, 0, s>>>(t->tv, a);
   return cuda_status(cudaGetLastError());
 }
 
@@ -455,7 +454,7 @@ int create_impl(mt_masstree** out, uint64_t pool_bytes, uint32_t tile_size) {
   const int one = 1;
   if (e == cudaSuccess) e = cudaMemcpy(p.slabs, root_img, sizeof(root_img), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(p.bump(0), &one, sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMallocHost(&t->h_err, 2 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&t->h_err, 4 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     cudaFree(t->mem);
     delete t;
@@ -650,12 +649,13 @@ int mt_scan(mt_masstree* t, const uint32_t* lower, const uint32_t* lower_lens, u
 int mt_sync(mt_masstree* t, void* stream) {
   if (!t) return MT_ERR_INVALID_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaMemcpyAsync(t->h_err, t->tv.pool.err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaMemcpyAsync(t->h_err, t->tv.pool.err, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return MT_ERR_CUDA;
   const uint32_t code = t->h_err[0];
   if (code != 0u) {
-    e = cudaMemsetAsync(t->tv.pool.err, 0, 3 * sizeof(uint32_t), s);
+    t->last_error_site = t->h_err[3];
+    e = cudaMemsetAsync(t->tv.pool.err, 0, 4 * sizeof(uint32_t), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return MT_ERR_CUDA;
   }
@@ -685,7 +685,7 @@ int mt_stats(mt_masstree* t, mt_stats_t* out) {
   const size_t nctr = (size_t)p.num_shards * 3u * kCtrStride;
   int* h = new (std::nothrow) int[nctr];
   if (!h) return MT_ERR_OOM;
-  uint32_t err[2] = {0, 0};
+  uint32_t err[4] = {0, 0, 0, 0};
   cudaError_t e = cudaMemcpy(h, p.ctr, nctr * sizeof(int), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(err, p.err, sizeof(err), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) { delete[] h; return MT_ERR_CUDA; }
@@ -707,6 +707,8 @@ int mt_stats(mt_masstree* t, mt_stats_t* out) {
   out->tile_size = t->tile_size;
   out->device_error = err[0];
   out->device_error_count = err[1];
+  out->device_error_site = err[0] ? err[3] : t->last_error_site;
+  out->reserved = 0;
   return MT_OK;
 }
 

@@ -183,7 +183,8 @@ struct mt_masstree {
   mtb::tree_view tv{};
   mtb::scan_frame* frames = nullptr;
   size_t frames_tiles = 0;
-  uint32_t* h_err = nullptr;  // pinned
+  uint32_t* h_err = nullptr;  // pinned: code, count, fatal flag, site of the first device error
+  uint32_t last_error_site = 0;  // site of the error the last mt_sync returned
   // Sub-batch scratch of mt_mixed_batches (see mt_batches.cu).
   void* batches_mem = nullptr;
   uint32_t batches_max_sub = 0;

@@ -40,7 +40,7 @@ MT_DEV bool find_parent(const tile<32>& t, const pool_view& p, uint32_t root, ui
   uint32_t idx = root, hops = 0;
   while (true) {
     if (!p.valid(idx) || ++hops > kMaxHops) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_MERGE));
       return false;
     }
     if (!nd.template load_verified<kConc>(t, p, idx)) return false;
@@ -49,7 +49,7 @@ MT_DEV bool find_parent(const tile<32>& t, const pool_view& p, uint32_t root, ui
     const int c = nd.child_pos(t, slice);
     const uint32_t ch = c < 0 ? kInvalid : nd.val_at(t, (uint32_t)c);
     if (!p.valid(ch)) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_MERGE));
       return false;
     }
     if (!cn.template load_verified<kConc>(t, p, ch)) return false;
@@ -91,7 +91,7 @@ MT_DEV void merge_one(const tile<32>& t, const pool_view& p, uint32_t root, uint
     if (i >= 1) {
       const uint32_t left = pn.val_at(t, (uint32_t)i - 1u);
       if (!p.valid(left) || !lock_load(t, p, left, a)) {
-        if (!p.valid(left) && t.leader()) record_error(p, ERR_CORRUPT);
+        if (!p.valid(left) && t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_MERGE));
         unlock_node(t, p, child);
         unlock_node(t, p, parent);
         return;
@@ -112,7 +112,7 @@ MT_DEV void merge_one(const tile<32>& t, const pool_view& p, uint32_t root, uint
     if ((uint32_t)i + 1u < n) {
       const uint32_t right = pn.val_at(t, (uint32_t)i + 1u);
       if (!p.valid(right) || !lock_load(t, p, right, a)) {
-        if (!p.valid(right) && t.leader()) record_error(p, ERR_CORRUPT);
+        if (!p.valid(right) && t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_MERGE));
         unlock_node(t, p, child);
         unlock_node(t, p, parent);
         return;
@@ -169,7 +169,7 @@ MT_DEV void remove_layers(const tile<32>& t, const tree_view& tv, const uint32_t
     }
     const uint32_t child = nd.val_at(t, (uint32_t)e);
     if (!p.valid(child) || !lock_load(t, p, child, cn)) {
-      if (!p.valid(child) && t.leader()) record_error(p, ERR_CORRUPT);
+      if (!p.valid(child) && t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_MERGE));
       unlock_node(t, p, nd.idx);
       return;
     }

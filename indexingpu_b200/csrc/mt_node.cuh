@@ -160,7 +160,7 @@ struct node {
       if constexpr (O == ld_order::NC) return true;
       if (tile_checksum(t) == word(t, WORD_CSUM)) return true;
     }
-    if (t.leader()) record_error(p, ERR_CORRUPT);
+    if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_NODE));
     return false;
   }
 

@@ -60,12 +60,18 @@ struct pool_view {
   MT_HD int* limbo_count(uint32_t s) const { return ctr + (size_t)(3u * s + 2u) * kCtrStride; }
 };
 
-// err[0] = first error code, err[1] = error count, err[2] = fatal flag.  A
+// Where an error was detected: a source file number (high 16 bits) and line.
+#define MT_AT(file) ((((uint32_t)(file)) << 16) | (uint32_t)__LINE__)
+enum mt_src_file : uint32_t { SRC_TREE = 1, SRC_NODE = 2, SRC_SUFFIX = 3, SRC_POOL = 4, SRC_FIND = 5, SRC_CAPI = 6,
+                              SRC_MERGE = 7, SRC_BULK = 8, SRC_SERVE = 9 };
+
+// err[0] = first error code, err[1] = error count, err[2] = fatal flag,
+// err[3] = where the first error was detected (MT_AT; 0 if not given).  A
 // fatal error (lock timeout, corruption, retry limit) makes every tile of the
 // launch stop taking new requests, so one failure cannot turn into a long
 // series of bounded waits.
-MT_DEV void record_error(const pool_view& p, uint32_t code) {
-  atomicCAS(p.err, 0u, code);
+MT_DEV void record_error(const pool_view& p, uint32_t code, uint32_t site = 0u) {
+  if (atomicCAS(p.err, 0u, code) == 0u) atomicExch(p.err + 3, site);
   atomicAdd(p.err + 1, 1u);
   if (code == ERR_LOCK_TIMEOUT || code == ERR_CORRUPT || code == ERR_RETRY_LIMIT) atomicExch(p.err + 2, 1u);
 }
@@ -136,7 +142,7 @@ struct slab_cache {
         if (count) shard = s;
       }
       if (count == 0) {
-        if (t.leader()) record_error(p, ERR_OOM);
+        if (t.leader()) record_error(p, ERR_OOM, MT_AT(SRC_POOL));
         return kInvalid;
       }
     }
@@ -150,10 +156,10 @@ struct slab_cache {
 
 // Retire one slab (called by one lane).  Safe to free after the current launch.
 MT_DEV void retire_slab(const pool_view& p, uint32_t slab) {
-  if (!p.valid(slab)) { record_error(p, ERR_CORRUPT); return; }
+  if (!p.valid(slab)) { record_error(p, ERR_CORRUPT, MT_AT(SRC_POOL)); return; }
   const uint32_t s = slab / p.shard_slabs;
   const int pos = atomicAdd(p.limbo_count(s), 1);
-  if (pos >= (int)p.shard_slabs) { record_error(p, ERR_CORRUPT); return; }
+  if (pos >= (int)p.shard_slabs) { record_error(p, ERR_CORRUPT, MT_AT(SRC_POOL)); return; }
   p.limbo[(size_t)s * p.shard_slabs + pos] = slab;
 }
 

@@ -24,6 +24,9 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -191,8 +194,16 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) server_kernel(tr
       // others, all in device memory, before it raises the request's flag
       // (the host reads results only through later copies or calls).
       const uint32_t f = atom_add_acq_rel_gpu_u32(sv.finished + it.req, 1u) + 1u;
-      if (f == it.items) st_relaxed_sys_u32(sv.done + it.req, 1u);
-      else if (f > it.items) record_error(tv.pool, ERR_CORRUPT);  // an item served twice
+      if (f == it.items) {
+        // The counter starts again at 0 for the next request of this slot
+        // (mt_server_* reuses slots); the system-scope fence makes every
+        // result of the request visible to the host's copies before the flag.
+        atomicExch(sv.finished + it.req, 0u);
+        __threadfence_system();
+        st_relaxed_sys_u32(sv.done + it.req, 1u);
+      } else if (f > it.items) {
+        record_error(tv.pool, ERR_CORRUPT, MT_AT(SRC_SERVE));  // an item served twice
+      }
     }
     // Warp-uniform: lane 0 reads the clock and decides for the whole warp
     // (every lane's own reading could split the warp).
@@ -274,12 +285,17 @@ X* mapped_alloc(size_t n, X** dev) {
 
 }  // namespace
 
+namespace {
+int serve_online(mt_masstree* t, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats);
+}  // namespace
+
 extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats) {
   if (!t || !plan || !latency_ns || plan->num_requests == 0 || !plan->request_first_op || !plan->request_num_ops ||
       !plan->arrival_ns || !plan->types || !plan->keys || !plan->values || !plan->value_lengths ||
       plan->max_key_length == 0 || plan->max_value_length == 0 ||
-      (plan->mode != MT_SERVE_SERVED && plan->mode != MT_SERVE_PLAIN))
+      (plan->mode != MT_SERVE_SERVED && plan->mode != MT_SERVE_PLAIN && plan->mode != MT_SERVE_ONLINE))
     return MT_ERR_INVALID_ARG;
+  if (plan->mode == MT_SERVE_ONLINE) return serve_online(t, plan, latency_ns, stats);
   const uint32_t nreq = plan->num_requests;
   uint64_t total_ops = 0;
   for (uint32_t r = 0; r < nreq; ++r) {
@@ -578,3 +594,575 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
   if (!rc) rc = mt_sync(t, nullptr);
   return rc;
 }
+
+// ---- online serving (mt_server_*) ------------------------------------------------------
+//
+// The device loop above, fed while it runs.  Clients call mt_server_submit
+// from any host thread; the server's own host thread (the pump) moves each
+// request through: queued -> admitted (staging space, a request slot and the
+// memory budget allow; ops uploaded on the upload stream) -> published (the
+// upload finished; work items on the ring) -> downloading (the device raised
+// the slot's completion flag; results copied to the client's buffers on the
+// download stream) -> done (copies finished; mt_server_poll reports it).
+// Staging is a ring of max_ops_in_flight ops filled and freed in admission
+// order; request slots are ticket % max_requests_in_flight.
+
+namespace {
+
+__global__ void fill_u32_kernel(uint32_t* p, uint32_t v, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+enum : uint32_t { SRV_UPLOADING = 0, SRV_PUBLISHED = 1, SRV_DOWNLOADING = 2, SRV_DONE = 3 };
+
+struct srv_request {
+  uint64_t ticket = 0;
+  const uint8_t* types = nullptr;
+  const uint32_t* keys = nullptr;
+  const uint32_t* klens = nullptr;
+  uint32_t* vals = nullptr;
+  uint32_t* vlens = nullptr;
+  bool* results = nullptr;
+  uint32_t n = 0;
+  uint64_t submit_ns = 0;
+  uint32_t off = 0;         // staging offset of the request's ops
+  uint64_t alloc_end = 0;   // staging head after its allocation
+  uint32_t demand = 0;      // slab demand estimate
+  uint32_t stage = SRV_UPLOADING;
+  cudaEvent_t ev = nullptr; // upload, then download
+};
+
+}  // namespace
+
+struct mt_server {
+  mt_masstree* tree = nullptr;
+  mt_server_config cfg{};
+  uint32_t C = 0, R = 0;
+  void* dmem = nullptr;
+  uint8_t* d_types = nullptr;
+  uint32_t *d_keys = nullptr, *d_klens = nullptr, *d_vals = nullptr, *d_vlens = nullptr, *d_order = nullptr;
+  bool* d_results = nullptr;
+  uint32_t* h_order = nullptr;  // pinned
+  serve_item *ring = nullptr, *d_ring = nullptr;
+  unsigned long long *pub = nullptr, *d_pub = nullptr;
+  uint32_t *stop = nullptr, *d_stop = nullptr, *done = nullptr, *d_done = nullptr;
+  unsigned long long *usage = nullptr, *d_usage = nullptr;
+  uint32_t* d_finished = nullptr;
+  server_ctl* d_ctl = nullptr;
+  unsigned long long* d_held = nullptr;
+  server_view sv{};
+  int blocks = 0;
+  size_t nwarps = 0;
+  cudaStream_t s_work = nullptr, s_up = nullptr, s_down = nullptr;
+  std::unique_ptr<std::atomic<uint64_t>[]> rec_ticket;
+  std::unique_ptr<std::atomic<uint32_t>[]> rec_done;
+  std::unique_ptr<std::atomic<uint64_t>[]> rec_latency;
+  std::vector<srv_request> slots;  // pump thread only
+  std::mutex mu;
+  std::deque<srv_request> queued;  // under mu
+  std::atomic<uint64_t> next_ticket{0};
+  std::thread pump;
+  std::atomic<bool> draining{false};  // stop asked: serve what is queued, then end
+  std::atomic<bool> quit{false};      // end now (the drain ran out of time)
+  std::atomic<bool> exited{false};    // the pump has ended
+  std::atomic<int> status{MT_OK};
+  clk::time_point t0;
+};
+
+namespace {
+
+void server_free(mt_server* S) {
+  if (S->s_work) cudaStreamSynchronize(S->s_work);
+  if (S->s_up) cudaStreamSynchronize(S->s_up);
+  if (S->s_down) cudaStreamSynchronize(S->s_down);
+  for (auto& r : S->slots)
+    if (r.ev) cudaEventDestroy(r.ev);
+  if (S->dmem) cudaFree(S->dmem);
+  if (S->h_order) cudaFreeHost(S->h_order);
+  for (void* h : {(void*)S->ring, (void*)S->pub, (void*)S->stop, (void*)S->done, (void*)S->usage})
+    if (h) cudaFreeHost(h);
+  if (S->d_finished) cudaFree(S->d_finished);
+  if (S->d_ctl) cudaFree(S->d_ctl);
+  if (S->d_held) cudaFree(S->d_held);
+  for (cudaStream_t st : {S->s_work, S->s_up, S->s_down})
+    if (st) cudaStreamDestroy(st);
+  delete S;
+}
+
+int copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind k, cudaStream_t s) {
+  if (bytes == 0) return MT_OK;
+  return cudaMemcpyAsync(dst, src, bytes, k, s) == cudaSuccess ? MT_OK : MT_ERR_CUDA;
+}
+
+// Upload request r into staging [r.off, r.off + r.n) on the upload stream.
+int server_upload(mt_server* S, srv_request& r) {
+  const uint32_t K = S->cfg.max_key_length, V = S->cfg.max_value_length, off = r.off, n = r.n;
+  // The request's ops grouped by kind (finds, inserts, updates, erases), so
+  // that the items cut from it mostly hold one kind (as in mt_serve).
+  uint32_t pos = off;
+  for (uint8_t kind : {(uint8_t)MT_REQ_FIND, (uint8_t)MT_REQ_INSERT, (uint8_t)MT_REQ_UPDATE, (uint8_t)MT_REQ_ERASE})
+    for (uint32_t o = 0; o < n; ++o)
+      if (r.types[o] == kind) S->h_order[pos++] = off + o;
+  for (uint32_t o = 0; o < n; ++o)
+    if (r.types[o] > MT_REQ_UPDATE) S->h_order[pos++] = off + o;  // served (and reported) last
+  cudaStream_t s = S->s_up;
+  int rc = copy_async(S->d_order + off, S->h_order + off, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
+  if (!rc) rc = copy_async(S->d_types + off, r.types, n, cudaMemcpyHostToDevice, s);
+  if (!rc) rc = copy_async(S->d_keys + (size_t)off * K, r.keys, (size_t)n * K * 4u, cudaMemcpyHostToDevice, s);
+  if (!rc && r.klens) rc = copy_async(S->d_klens + off, r.klens, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
+  if (!rc && !r.klens) {
+    fill_u32_kernel<<<std::max(1u, std::min(64u, (n + 255u) / 256u)), 256, 0, s>>>(S->d_klens + off, K, n);
+    rc = cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
+  }
+  if (!rc) rc = copy_async(S->d_vals + (size_t)off * V, r.vals, (size_t)n * V * 4u, cudaMemcpyHostToDevice, s);
+  if (!rc) rc = copy_async(S->d_vlens + off, r.vlens, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
+  if (!rc && cudaEventRecord(r.ev, s) != cudaSuccess) rc = MT_ERR_CUDA;
+  return rc;
+}
+
+int server_download(mt_server* S, srv_request& r) {
+  const uint32_t V = S->cfg.max_value_length, off = r.off, n = r.n;
+  cudaStream_t s = S->s_down;
+  int rc = copy_async(r.vals, S->d_vals + (size_t)off * V, (size_t)n * V * 4u, cudaMemcpyDeviceToHost, s);
+  if (!rc) rc = copy_async(r.vlens, S->d_vlens + off, (size_t)n * 4u, cudaMemcpyDeviceToHost, s);
+  if (!rc && r.results) rc = copy_async(r.results, S->d_results + off, n, cudaMemcpyDeviceToHost, s);
+  if (!rc && cudaEventRecord(r.ev, s) != cudaSuccess) rc = MT_ERR_CUDA;
+  return rc;
+}
+
+void server_pump(mt_server* S) {
+  mt_masstree* t = S->tree;
+  if (cudaSetDevice(t->device) != cudaSuccess) { S->status = MT_ERR_CUDA; return; }
+  const uint32_t C = S->C, R = S->R;
+  const uint32_t tiles_per_warp = 32u / t->tile_size;
+  const uint64_t total_tiles = S->nwarps * tiles_per_warp;
+  const bool auto_chunk = S->cfg.chunk_ops == 0;
+  const uint32_t fixed_chunk = std::max<uint32_t>(1u, std::min<uint32_t>(S->cfg.chunk_ops, 4096u));
+  const double budget = S->cfg.memory_budget > 0.f ? S->cfg.memory_budget : 0.9;
+  const unsigned long long epoch_ns = (unsigned long long)(S->cfg.epoch_us ? S->cfg.epoch_us : 20000u) * 1000ull;
+  const uint32_t per_write = 1u + suf_nodes(S->cfg.max_key_length, S->cfg.max_value_length);
+  mt_stats_t st{};
+  if (mt_stats(t, &st) != MT_OK) { S->status = MT_ERR_CUDA; return; }
+  const double slab_budget = budget * (double)st.total_slabs;
+  double slabs_in_use = (double)st.used_slabs + (double)st.limbo_slabs;
+  uint64_t admitted_demand = 0, completed_demand = 0;
+
+  std::deque<uint32_t> fifo, upq, downq;  // slots, in admission / upload / download order
+  std::vector<uint32_t> published;        // slots waiting for the device
+  uint64_t head = 0, tail = 0;            // staging ring (ops)
+  uint64_t items_published = 0, admitted_ops = 0, completed_ops = 0;
+  std::vector<cudaEvent_t> evs;
+  std::vector<uint64_t> enq_completed;
+  size_t ev_done = 0;
+  auto enqueue_epoch = [&]() -> int {
+    int r2 = host_launch_reclaim(t, S->s_work);
+    if (r2) return r2;
+    pool_usage_kernel<<<1, 32, 0, S->s_work>>>(t->tv.pool, S->d_usage);
+    r2 = launch_server_tile(t, S->blocks, S->sv, epoch_ns, S->s_work);
+    if (r2) return r2;
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return MT_ERR_CUDA;
+    if (cudaEventRecord(e, S->s_work) != cudaSuccess) return MT_ERR_CUDA;
+    evs.push_back(e);
+    enq_completed.push_back(completed_demand);
+    return MT_OK;
+  };
+  int rc = enqueue_epoch();
+  if (!rc) rc = enqueue_epoch();
+  uint64_t stuck_since = 0;
+  while (!rc) {
+    bool progress = false;
+    // ---- admit queued requests in order --------------------------------------
+    while (true) {
+      srv_request r;
+      {
+        std::lock_guard<std::mutex> g(S->mu);
+        if (S->queued.empty()) break;
+        const srv_request& f = S->queued.front();
+        const uint64_t oldest = fifo.empty() ? f.ticket : S->slots[fifo.front()].ticket;
+        if (f.ticket - oldest >= R) break;  // no free request slot
+        uint64_t h = head;
+        if (h % C + f.n > C) h += C - h % C;  // the request's ops stay contiguous
+        if (h + f.n - tail > C) break;        // no staging space
+        uint32_t d = 0;
+        for (uint32_t o = 0; o < f.n; ++o)
+          d += (f.types[o] == MT_REQ_INSERT || f.types[o] == MT_REQ_UPDATE) ? per_write : 0u;
+        if (slabs_in_use + d > slab_budget) {
+          // Admission waits for memory (slabs come back between launches).
+          if (fifo.empty()) {
+            const uint64_t now = now_ns(S->t0);
+            if (!stuck_since) stuck_since = now;
+            else if (now - stuck_since > 60ull * 1000000000ull) rc = MT_ERR_OOM;  // never fits
+          }
+          break;
+        }
+        stuck_since = 0;
+        r = f;
+        S->queued.pop_front();
+        r.off = (uint32_t)(h % C);
+        head = h + r.n;
+        r.alloc_end = head;
+        r.demand = d;
+      }
+      const uint32_t slot = (uint32_t)(r.ticket % R);
+      srv_request& q = S->slots[slot];
+      r.ev = q.ev;
+      r.stage = SRV_UPLOADING;
+      q = r;
+      S->rec_done[slot].store(0u, std::memory_order_relaxed);
+      S->rec_ticket[slot].store(r.ticket, std::memory_order_release);
+      slabs_in_use += r.demand;
+      admitted_demand += r.demand;
+      admitted_ops += r.n;
+      rc = server_upload(S, q);
+      if (rc) break;
+      fifo.push_back(slot);
+      upq.push_back(slot);
+      progress = true;
+    }
+    // ---- publish uploaded requests as work items -------------------------------
+    while (!rc && !upq.empty() && cudaEventQuery(S->slots[upq.front()].ev) == cudaSuccess) {
+      const uint32_t slot = upq.front();
+      upq.pop_front();
+      srv_request& q = S->slots[slot];
+      uint32_t chunk = fixed_chunk;
+      if (auto_chunk) {
+        const uint64_t backlog = admitted_ops - std::min(admitted_ops, completed_ops);
+        const uint64_t per_tile = backlog / total_tiles;
+        chunk = backlog < S->nwarps / 8 ? 1u
+                                         : tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
+      }
+      const uint32_t n_items = std::max<uint32_t>(1u, (q.n + chunk - 1) / chunk);
+      S->done[slot] = 0u;
+      uint32_t f = q.off, left = q.n;
+      for (uint32_t k = 0; k < n_items; ++k) {
+        const uint32_t c = std::min(left, chunk);
+        S->ring[items_published % C] = serve_item{slot, f, c, n_items};
+        ++items_published;
+        f += c;
+        left -= c;
+      }
+      __atomic_store_n(S->pub, (unsigned long long)items_published, __ATOMIC_RELEASE);
+      q.stage = SRV_PUBLISHED;
+      published.push_back(slot);
+      progress = true;
+    }
+    // ---- completed on the device: download the results --------------------------
+    for (size_t k = 0; !rc && k < published.size();) {
+      const uint32_t slot = published[k];
+      if (__atomic_load_n(&S->done[slot], __ATOMIC_ACQUIRE)) {
+        srv_request& q = S->slots[slot];
+        rc = server_download(S, q);
+        q.stage = SRV_DOWNLOADING;
+        downq.push_back(slot);
+        published[k] = published.back();
+        published.pop_back();
+        progress = true;
+      } else {
+        ++k;
+      }
+    }
+    // ---- downloads finished: the tickets are done -------------------------------
+    while (!rc && !downq.empty() && cudaEventQuery(S->slots[downq.front()].ev) == cudaSuccess) {
+      const uint32_t slot = downq.front();
+      downq.pop_front();
+      srv_request& q = S->slots[slot];
+      q.stage = SRV_DONE;
+      completed_demand += q.demand;
+      completed_ops += q.n;
+      S->rec_latency[slot].store(now_ns(S->t0) - q.submit_ns, std::memory_order_relaxed);
+      S->rec_done[slot].store(1u, std::memory_order_release);
+      progress = true;
+    }
+    while (!fifo.empty() && S->slots[fifo.front()].stage == SRV_DONE) {
+      tail = S->slots[fifo.front()].alloc_end > tail ? S->slots[fifo.front()].alloc_end : tail;
+      fifo.pop_front();
+    }
+    // ---- keep the device loop running -------------------------------------------
+    while (!rc && ev_done < evs.size() && cudaEventQuery(evs[ev_done]) == cudaSuccess) {
+      ++ev_done;
+      rc = enqueue_epoch();
+      // Retired slabs came back with the reclaim pass before that launch:
+      // restart the estimate from the pool count taken then, plus the demand
+      // of every request not complete when that epoch was enqueued.
+      slabs_in_use = (double)__atomic_load_n(S->usage, __ATOMIC_ACQUIRE) +
+                     (double)(admitted_demand - std::min(admitted_demand, enq_completed[ev_done - 1]));
+      if (ev_done > 64) {  // events of finished epochs
+        for (size_t k = 0; k + 2 < ev_done; ++k) cudaEventDestroy(evs[k]);
+        evs.erase(evs.begin(), evs.begin() + (ev_done - 2));
+        enq_completed.erase(enq_completed.begin(), enq_completed.begin() + (ev_done - 2));
+        ev_done = 2;
+      }
+    }
+    if (S->quit.load(std::memory_order_acquire)) break;
+    if (S->draining.load(std::memory_order_acquire) && fifo.empty()) {
+      std::lock_guard<std::mutex> g(S->mu);
+      if (S->queued.empty()) break;
+    }
+    if (!progress) std::this_thread::yield();
+  }
+  // The device loop leaves at the stop flag (or its launch's time budget).
+  __atomic_store_n(S->stop, 1u, __ATOMIC_RELEASE);
+  cudaStreamSynchronize(S->s_work);
+  cudaStreamSynchronize(S->s_up);
+  cudaStreamSynchronize(S->s_down);
+  for (auto e : evs) cudaEventDestroy(e);
+  if (rc) S->status = rc;
+  S->exited.store(true, std::memory_order_release);
+}
+
+}  // namespace
+
+extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_server** out) {
+  if (!t || !cfg || !out || cfg->max_key_length == 0 || cfg->max_value_length == 0) return MT_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (cudaSetDevice(t->device) != cudaSuccess) return MT_ERR_CUDA;
+  auto* S = new (std::nothrow) mt_server();
+  if (!S) return MT_ERR_OOM;
+  S->tree = t;
+  S->cfg = *cfg;
+  S->C = cfg->max_ops_in_flight ? cfg->max_ops_in_flight : (1u << 20);
+  S->R = cfg->max_requests_in_flight ? cfg->max_requests_in_flight : 65536u;
+  const uint32_t C = S->C, R = S->R, K = cfg->max_key_length, V = cfg->max_value_length;
+  auto up = [](size_t b) { return (b + 255u) & ~size_t(255); };
+  const size_t bytes = up(C) + up((size_t)C * K * 4u) + 3 * up((size_t)C * 4u) + up((size_t)C * V * 4u) + up(C);
+  bool ok = cudaMalloc(&S->dmem, bytes) == cudaSuccess;
+  if (ok) {
+    char* p = static_cast<char*>(S->dmem);
+    S->d_types = reinterpret_cast<uint8_t*>(p); p += up(C);
+    S->d_keys = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * K * 4u);
+    S->d_klens = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
+    S->d_vlens = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
+    S->d_order = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
+    S->d_vals = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * V * 4u);
+    S->d_results = reinterpret_cast<bool*>(p);
+  }
+  ok = ok && cudaMallocHost(&S->h_order, (size_t)C * 4u) == cudaSuccess;
+  if (ok) {
+    S->ring = mapped_alloc<serve_item>(C, &S->d_ring);
+    S->pub = mapped_alloc<unsigned long long>(1, &S->d_pub);
+    S->stop = mapped_alloc<uint32_t>(1, &S->d_stop);
+    S->done = mapped_alloc<uint32_t>(R, &S->d_done);
+    S->usage = mapped_alloc<unsigned long long>(1, &S->d_usage);
+    ok = S->ring && S->pub && S->stop && S->done && S->usage;
+  }
+  S->blocks = server_blocks_tile(t);
+  S->nwarps = (size_t)S->blocks * (kBlock / 32);
+  ok = ok && cudaMalloc(&S->d_finished, (size_t)R * 4u) == cudaSuccess &&
+       cudaMemset(S->d_finished, 0, (size_t)R * 4u) == cudaSuccess &&
+       cudaMalloc(&S->d_ctl, sizeof(server_ctl)) == cudaSuccess &&
+       cudaMemset(S->d_ctl, 0, sizeof(server_ctl)) == cudaSuccess &&
+       cudaMalloc(&S->d_held, S->nwarps * sizeof(unsigned long long)) == cudaSuccess &&
+       cudaMemset(S->d_held, 0xFF, S->nwarps * sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&S->s_work, cudaStreamNonBlocking) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&S->s_up, cudaStreamNonBlocking) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&S->s_down, cudaStreamNonBlocking) == cudaSuccess;
+  if (ok) {
+    S->slots.resize(R);
+    for (auto& r : S->slots) ok = ok && cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming) == cudaSuccess;
+    S->rec_ticket.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
+    S->rec_done.reset(new (std::nothrow) std::atomic<uint32_t>[R]);
+    S->rec_latency.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
+    ok = ok && S->rec_ticket && S->rec_done && S->rec_latency;
+    for (uint32_t k = 0; ok && k < R; ++k) {
+      S->rec_ticket[k].store(0);
+      S->rec_done[k].store(0);
+      S->rec_latency[k].store(0);
+    }
+  }
+  if (!ok) {
+    server_free(S);
+    return MT_ERR_OOM;
+  }
+  server_view& sv = S->sv;
+  sv.ring = S->d_ring;
+  sv.published = S->d_pub;
+  sv.stop = S->d_stop;
+  sv.ctl = S->d_ctl;
+  sv.held = S->d_held;
+  sv.finished = S->d_finished;
+  sv.done = S->d_done;
+  sv.ring_cap = C;
+  sv.order = S->d_order;
+  batch_args ops{};
+  ops.types = S->d_types;
+  ops.keys = S->d_keys;
+  ops.key_lengths = S->d_klens;
+  ops.values = S->d_vals;
+  ops.value_lengths_in = S->d_vlens;
+  ops.value_lengths_out = S->d_vlens;
+  ops.results = S->d_results;
+  ops.max_key_length = K;
+  ops.max_value_length = V;
+  sv.ops = ops;
+  // Every earlier call on the tree finishes first; one launch without a time
+  // budget loads the kernel and leaves every warp holding its first ticket.
+  *S->usage = 0;
+  ok = cudaDeviceSynchronize() == cudaSuccess && host_launch_reclaim(t, S->s_work) == MT_OK &&
+       launch_server_tile(t, S->blocks, sv, 0ull, S->s_work) == MT_OK &&
+       cudaStreamSynchronize(S->s_work) == cudaSuccess;
+  if (!ok) {
+    server_free(S);
+    return MT_ERR_CUDA;
+  }
+  S->t0 = clk::now();
+  S->pump = std::thread(server_pump, S);
+  *out = S;
+  return MT_OK;
+}
+
+extern "C" int mt_server_submit(mt_server* S, const uint8_t* types, const uint32_t* keys, const uint32_t* klens,
+                                uint32_t* vals, uint32_t* vlens, bool* results, uint32_t n, uint64_t* ticket) {
+  if (!S || !ticket || n == 0 || n > S->C || !types || !keys || !vals || !vlens) return MT_ERR_INVALID_ARG;
+  if (S->draining.load(std::memory_order_acquire)) return MT_ERR_INVALID_ARG;
+  const int st = S->status.load(std::memory_order_acquire);
+  if (st) return st;
+  srv_request r;
+  r.types = types;
+  r.keys = keys;
+  r.klens = klens;
+  r.vals = vals;
+  r.vlens = vlens;
+  r.results = results;
+  r.n = n;
+  std::lock_guard<std::mutex> g(S->mu);
+  r.submit_ns = now_ns(S->t0);
+  r.ticket = S->next_ticket.load(std::memory_order_relaxed);
+  S->queued.push_back(r);
+  S->next_ticket.store(r.ticket + 1, std::memory_order_release);
+  *ticket = r.ticket;
+  return MT_OK;
+}
+
+extern "C" int mt_server_poll(mt_server* S, uint64_t ticket, int* done, uint64_t* latency_ns) {
+  if (!S || !done || ticket >= S->next_ticket.load(std::memory_order_acquire)) return MT_ERR_INVALID_ARG;
+  const uint32_t slot = (uint32_t)(ticket % S->R);
+  const uint64_t rt = S->rec_ticket[slot].load(std::memory_order_acquire);
+  *done = 0;
+  if (latency_ns) *latency_ns = 0;
+  if (rt > ticket) {
+    *done = 1;  // the slot moved on to a later request: this one completed (its latency is gone)
+  } else if (rt == ticket && S->rec_done[slot].load(std::memory_order_acquire)) {
+    *done = 1;
+    if (latency_ns) *latency_ns = S->rec_latency[slot].load(std::memory_order_relaxed);
+  }
+  if (!*done) {
+    const int st = S->status.load(std::memory_order_acquire);
+    if (st) return st;
+  }
+  return MT_OK;
+}
+
+extern "C" int mt_server_stop(mt_server* S) {
+  if (!S) return MT_ERR_INVALID_ARG;
+  // Serve what is queued; bound the wait, then end the loop regardless.
+  S->draining.store(true, std::memory_order_release);
+  const auto deadline = clk::now() + std::chrono::seconds(60);
+  while (!S->exited.load(std::memory_order_acquire) && clk::now() < deadline)
+    std::this_thread::sleep_for(std::chrono::microseconds(100));
+  const bool drained = S->exited.load(std::memory_order_acquire);
+  S->quit.store(true, std::memory_order_release);
+  if (S->pump.joinable()) S->pump.join();
+  int rc = S->status.load();
+  if (!rc && !drained) rc = MT_ERR_LOCK_TIMEOUT;
+  mt_masstree* t = S->tree;
+  server_free(S);
+  const int dev_rc = mt_sync(t, nullptr);
+  return rc ? rc : dev_rc;
+}
+
+namespace {
+
+// MT_SERVE_ONLINE: replay of an open-loop plan through mt_server_*.  Requests
+// are submitted in arrival order, each when its arrival time has come, from
+// host buffers; a poller thread records when each one is done.  Latency is
+// done - arrival (the submit call, the upload, the device work and the
+// download of the results).
+int serve_online(mt_masstree* t, const mt_serve_plan* plan, uint64_t* latency_ns, mt_serve_stats* stats) {
+  const uint32_t nreq = plan->num_requests;
+  uint32_t max_ops = 1;
+  for (uint32_t r = 0; r < nreq; ++r) {
+    if (r > 0 && plan->arrival_ns[r] < plan->arrival_ns[r - 1]) return MT_ERR_INVALID_ARG;
+    if (plan->request_num_ops[r] == 0) return MT_ERR_INVALID_ARG;
+    max_ops = std::max(max_ops, plan->request_num_ops[r]);
+  }
+  mt_server_config cfg{};
+  cfg.max_key_length = plan->max_key_length;
+  cfg.max_value_length = plan->max_value_length;
+  cfg.max_ops_in_flight = std::max<uint32_t>(1u << 20, max_ops);
+  cfg.chunk_ops = plan->chunk_ops;
+  cfg.epoch_us = plan->epoch_us;
+  cfg.memory_budget = plan->memory_budget;
+  mt_server* S = nullptr;
+  int rc = mt_server_start(t, &cfg, &S);
+  if (rc) return rc;
+  std::vector<uint64_t> tickets(nreq, ~0ull), submitted(nreq, 0), completion(nreq, 0);
+  std::atomic<uint32_t> n_submitted{0};
+  std::atomic<bool> submit_end{false};
+  std::atomic<bool> poll_fail{false};
+  const clk::time_point t0 = clk::now();
+  std::thread poller([&] {
+    uint32_t next = 0;
+    std::vector<uint32_t> pending;
+    while (true) {
+      const bool ended = submit_end.load(std::memory_order_acquire);
+      const uint32_t ns = n_submitted.load(std::memory_order_acquire);
+      if (ended && next == ns && pending.empty()) break;
+      while (next < ns) pending.push_back(next++);
+      bool progress = false;
+      for (size_t k = 0; k < pending.size();) {
+        int d = 0;
+        if (mt_server_poll(S, tickets[pending[k]], &d, nullptr) != MT_OK) {
+          poll_fail = true;
+          return;
+        }
+        if (d) {
+          completion[pending[k]] = now_ns(t0);
+          pending[k] = pending.back();
+          pending.pop_back();
+          progress = true;
+        } else {
+          ++k;
+        }
+      }
+      if (now_ns(t0) > plan->arrival_ns[nreq - 1] + 60ull * 1000000000ull) {
+        poll_fail = true;
+        return;
+      }
+      if (!progress) std::this_thread::yield();
+    }
+  });
+  for (uint32_t r = 0; r < nreq && !rc && !poll_fail; ++r) {
+    while (now_ns(t0) < plan->arrival_ns[r]) {
+    }
+    const uint32_t f = plan->request_first_op[r], n = plan->request_num_ops[r];
+    rc = mt_server_submit(S, plan->types + f, plan->keys + (size_t)f * plan->max_key_length,
+                          plan->key_lengths ? plan->key_lengths + f : nullptr,
+                          plan->values + (size_t)f * plan->max_value_length, plan->value_lengths + f,
+                          plan->results ? plan->results + f : nullptr, n, &tickets[r]);
+    submitted[r] = now_ns(t0);
+    if (!rc) n_submitted.store(r + 1, std::memory_order_release);
+  }
+  submit_end.store(true, std::memory_order_release);
+  poller.join();
+  const int stop_rc = mt_server_stop(S);
+  uint64_t ops_done = 0, end = 0, done_req = 0;
+  for (uint32_t r = 0; r < nreq; ++r) {
+    latency_ns[r] = completion[r] ? completion[r] - std::min(completion[r], plan->arrival_ns[r]) : 0ull;
+    if (completion[r]) {
+      ops_done += plan->request_num_ops[r];
+      ++done_req;
+    }
+    end = std::max<uint64_t>(end, completion[r]);
+  }
+  if (stats) {
+    stats->wall_ns = end;
+    stats->requests_done = done_req;
+    stats->ops_done = ops_done;
+    stats->admission_waits = 0;
+  }
+  if (!rc && poll_fail) rc = MT_ERR_LOCK_TIMEOUT;
+  return rc ? rc : stop_rc;
+}
+
+}  // namespace

@@ -228,12 +228,12 @@ MT_DEV void suffix_retire(const tile<T>& t, const pool_view& p, uint32_t head) {
     const uint32_t nn = suf_nodes(hdr & kMaxLen16, hdr >> 16);
     uint32_t c = head;
     for (uint32_t q = 0; q < nn; ++q) {
-      if (!p.valid(c)) { record_error(p, ERR_CORRUPT); break; }
+      if (!p.valid(c)) { record_error(p, ERR_CORRUPT, MT_AT(SRC_SUFFIX)); break; }
       const uint32_t nx = ld_word<O>(p.addr(c) + SUF_WORD_NEXT);
       retire_slab(p, c);
       c = nx;
     }
-    if (c != kInvalid) record_error(p, ERR_CORRUPT);
+    if (c != kInvalid) record_error(p, ERR_CORRUPT, MT_AT(SRC_SUFFIX));
   }
   t.sync();
 }

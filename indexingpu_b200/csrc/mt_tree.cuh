@@ -101,8 +101,8 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
     old = t.shfl(old, 0);
     if (!(old & META_LOCK)) {
       t.sync();
-      // The previous holder's image may still be landing (its publishing
-      // store also released the lock): reload until the checksum matches.
+      // No writer can publish this node while we hold its lock; a checksum
+      // mismatch here would be a bug, reported as corruption.
       return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
@@ -110,7 +110,7 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
     __nanosleep(backoff + ((jitter >> 16) & (backoff - 1u)));
     if (backoff < 512u) backoff <<= 1;
   }
-  if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT);
+  if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT, MT_AT(SRC_TREE));
   return false;
 }
 
@@ -123,19 +123,16 @@ MT_DEV void publish_locked(const tile<T>& t, const pool_view& p, node<T>& nd) {
   nd.template store<st_order::RELEASE>(t, p);
 }
 
-// Publish the node image and release its lock with the same line store (the
-// stored meta word has LOCK clear): one release store instead of a store and
-// a release atomic.  The next locker reloads the node after its lock atomic
-// and accepts only an image whose checksum (which covers the version) matches,
-// so it never works on a mix of this image and the one before; each of its
-// lanes then stores the words it loaded, after the values it read
-// (per-location coherence), so no word of this image is lost.
+// Publish the node image, then release its lock.  The release is a separate
+// atomic after the image store (release-ordered): a line store is not seen
+// atomically on B200, and a next holder must not take the lock before every
+// word of this image has landed.  (Clearing LOCK in the image store itself,
+// which saves the atomic, produced corrupted nodes under contention.)
 template <int T>
 MT_DEV void publish_unlock(const tile<T>& t, const pool_view& p, node<T>& nd) {
-  nd.meta = (nd.meta & ~META_LOCK) + META_VERSION_ONE;
-  nd.encode_header(t);
-  nd.seal(t);
-  nd.template store<st_order::RELEASE>(t, p);
+  publish_locked(t, p, nd);
+  unlock_node(t, p, nd.idx);
+  nd.meta &= ~META_LOCK;
 }
 
 // Write a node that no other tile can reach yet.
@@ -166,7 +163,7 @@ MT_DEV bool descend(const tile<T>& t, const pool_view& p, uint32_t root, uint32_
   uint32_t idx = root;
   while (true) {
     if (!p.valid(idx) || ++hops > hop_limit) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE));
       return false;
     }
     if (!nd.template load_verified<O>(t, p, idx)) return false;
@@ -174,7 +171,7 @@ MT_DEV bool descend(const tile<T>& t, const pool_view& p, uint32_t root, uint32_
     if (nd.is_border()) return true;
     const int c = nd.child_pos(t, slice);
     if (c < 0) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE));
       return false;
     }
     idx = nd.val_at(t, (uint32_t)c);
@@ -188,7 +185,7 @@ MT_DEV bool lock_border(const tile<T>& t, const pool_view& p, uint32_t slice, no
   uint32_t idx = nd.idx;
   while (true) {
     if (!p.valid(idx) || ++hops > kMaxHops) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE));
       return false;
     }
     if (!lock_load(t, p, idx, nd)) return false;
@@ -276,7 +273,7 @@ MT_DEV int split_full(const tile<T>& t, const pool_view& p, slab_cache<T>& cache
   } else {
     if (parent == kInvalid || ++restarts > kMaxRestarts) {
       unlock_node(t, p, idx);
-      if (restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+      if (restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT, MT_AT(SRC_TREE)); return -1; }
       return 1;
     }
     node<T> pn;
@@ -286,7 +283,7 @@ MT_DEV int split_full(const tile<T>& t, const pool_view& p, slab_cache<T>& cache
       // The parent changed under us: start the layer again.
       unlock_node(t, p, parent);
       unlock_node(t, p, idx);
-      if (++restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT); return -1; }
+      if (++restarts > kMaxRestarts) { if (t.leader()) record_error(p, ERR_RETRY_LIMIT, MT_AT(SRC_TREE)); return -1; }
       return 1;
     }
     const uint32_t R = cache.allocate(t, p);
@@ -335,7 +332,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
   uint32_t restarts = 0;
   while (true) {
     if (!p.valid(idx) || ++hops > kMaxHops) {
-      if (t.leader()) record_error(p, ERR_CORRUPT);
+      if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE));
       return -1;
     }
     if (!nd.template load_verified<kConc>(t, p, idx)) return -1;
@@ -346,7 +343,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
     }
     if (!nd.is_border() && !nd.full()) {
       const int c = nd.child_pos(t, slice);
-      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return -1; }
       parent = idx;
       idx = nd.val_at(t, (uint32_t)c);
       continue;
@@ -358,7 +355,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
       if (nd.is_border()) return 0;
       unlock_node(t, p, idx);
       const int c = nd.child_pos(t, slice);
-      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+      if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return -1; }
       parent = idx;
       idx = nd.val_at(t, (uint32_t)c);
       continue;
@@ -366,7 +363,16 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
     // nd is full and locked: split it.
     const int sr = split_full(t, p, cache, slice, nd, parent, restarts);
     if (sr < 0) return -1;
-    if (sr == 1) { idx = root; parent = kInvalid; continue; }
+    if (sr == 1) {
+      // Start the layer again.  The node-visit bound (which catches cycles)
+      // applies per attempt; attempts are bounded by kMaxRestarts.  Inserts
+      // into a young tree, where every tile meets the same splitting nodes,
+      // restart thousands of times.
+      idx = root;
+      parent = kInvalid;
+      hops = 0;
+      continue;
+    }
     // nd is now the non-full half covering slice; locked iff border.
     if (nd.is_border()) {
       nd.meta |= META_LOCK;
@@ -374,7 +380,7 @@ MT_DEV int descend_split(const tile<T>& t, const pool_view& p, slab_cache<T>& ca
     }
     if (nd.locked()) unlock_node(t, p, nd.idx);
     const int c = nd.child_pos(t, slice);
-    if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT); return -1; }
+    if (c < 0) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return -1; }
     parent = nd.idx;
     idx = nd.val_at(t, (uint32_t)c);
   }
@@ -403,7 +409,7 @@ MT_DEV uint32_t coop_find(const tile<T>& t, const tree_view& tv, const uint32_t*
       if (maxV > 0u && out != nullptr && t.leader()) out[0] = v;
       return 1u;
     }
-    if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT); return 0u; }
+    if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return 0u; }
     suffix_head<T> h;
     h.template load<OS>(t, p, v);
     if (st == KS_SUFFIX) {
@@ -552,7 +558,7 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
                        uint32_t klen, const uint32_t* val, uint32_t vlen) {
   const pool_view& p = tv.pool;
   if (klen == 0u || vlen > kMaxLen16 || klen > kMaxLen16) {
-    if (t.leader()) record_error(p, ERR_INVALID_ARG);
+    if (t.leader()) record_error(p, ERR_INVALID_ARG, MT_AT(SRC_TREE));
     return RES_ERR;
   }
   uint32_t root = tv.root, hops = 0;
@@ -574,7 +580,7 @@ MT_DEV int coop_insert(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
         return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
       }
       // SUFFIX entry: same key, or a different key sharing this slice.
-      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return RES_ERR; }
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);
       const uint32_t lk = klen - layer - 1u;
@@ -638,7 +644,7 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
                        uint32_t klen, const uint32_t* val, uint32_t vlen) {
   const pool_view& p = tv.pool;
   if (klen == 0u || vlen > kMaxLen16) {
-    if (t.leader()) record_error(p, ERR_INVALID_ARG);
+    if (t.leader()) record_error(p, ERR_INVALID_ARG, MT_AT(SRC_TREE));
     return RES_ERR;
   }
   uint32_t root = tv.root, hops = 0;
@@ -660,7 +666,7 @@ MT_DEV int coop_update(const tile<T>& t, const tree_view& tv, slab_cache<T>& cac
     const uint32_t v = nd.val_at(t, (uint32_t)e);
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
     if (st == KS_VALUE || st == KS_LONGVAL) return replace_value(t, p, cache, nd, (uint32_t)e, st, v, val, vlen);
-    if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
+    if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return RES_ERR; }
     const uint32_t lk = klen - layer - 1u;
     if (v != v0) {  // the chain changed since the lock-free check: compare again
       suffix_head<T> h;
@@ -700,7 +706,7 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
     const uint32_t v = nd.val_at(t, (uint32_t)e);
     if (st == KS_LINK) { unlock_node(t, p, nd.idx); root = v; ++layer; continue; }
     if (st == KS_SUFFIX && v != v0) {
-      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT); return RES_ERR; }
+      if (!p.valid(v)) { unlock_node(t, p, nd.idx); if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return RES_ERR; }
       suffix_head<T> h;
       h.template load<kConcSuffix>(t, p, v);
       const uint32_t lk = klen - layer - 1u;
@@ -785,7 +791,7 @@ struct scan_frames {
     shrink_to(t, p, i);
     if (cur == kInvalid || i >= base + kFramesPerSlab) {
       if (cache == nullptr) {
-        if (t.leader()) record_error(p, ERR_KEY_TOO_LONG);
+        if (t.leader()) record_error(p, ERR_KEY_TOO_LONG, MT_AT(SRC_TREE));
         return false;
       }
       const uint32_t s = cache->allocate(t, p);
@@ -946,7 +952,7 @@ MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint
       suffix_head<T> h;
       const bool has_chain = st == KS_SUFFIX || st == KS_LONGVAL;
       if (has_chain) {
-        if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+        if (!p.valid(v)) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return count; }
         h.template load<OS>(t, p, v);
       }
       if (ltight) {
@@ -1001,7 +1007,7 @@ MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint
     if (nd.has_sib()) {
       if (utight && nd.high >= upper[layer]) return count;
       const uint32_t sib = nd.sib;
-      if (!p.valid(sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+      if (!p.valid(sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return count; }
       if (!nd.template load_verified<O>(t, p, sib)) return count;
       start = 0;
       continue;
@@ -1020,10 +1026,10 @@ MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint
       start = 0;
       continue;
     }
-    if (!p.valid(f.node)) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+    if (!p.valid(f.node)) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return count; }
     if (!nd.template load_verified<O>(t, p, f.node)) return count;
     while (nd.must_move_right(f.slice)) {
-      if (!p.valid(nd.sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT); return count; }
+      if (!p.valid(nd.sib) || ++hops > hop_limit) { if (t.leader()) record_error(p, ERR_CORRUPT, MT_AT(SRC_TREE)); return count; }
       if (!nd.template load_verified<O>(t, p, nd.sib)) return count;
     }
     start = __popc(nd.entry_mask(t, [&](uint32_t k, uint32_t) { return k <= f.slice; }));

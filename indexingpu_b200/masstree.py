@@ -35,9 +35,11 @@ STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORR
 
 
 class MasstreeError(RuntimeError):
-    def __init__(self, code, what):
+    def __init__(self, code, what, site=0):
         self.code = code
-        super().__init__(f"{what}: {STATUS.get(code, code)}")
+        self.site = site
+        where = f" (detected at source file {site >> 16}, line {site & 0xFFFF})" if site else ""
+        super().__init__(f"{what}: {STATUS.get(code, code)}{where}")
 
 
 def _ptr(x):
@@ -45,7 +47,9 @@ def _ptr(x):
         return None
     if isinstance(x, int):
         return x or None
-    return x.data_ptr()
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data  # numpy
 
 
 def _stream(s):
@@ -195,12 +199,14 @@ class GpuMasstree:
     # -- serving ---------------------------------------------------------------------
     def serve(self, types, keys, max_key_length, key_lengths, values, max_value_length, value_lengths, results,
               request_first_op, request_num_ops, arrival_ns, plain=False, chunk_ops=0, epoch_us=0,
-              memory_budget=0.0):
+              memory_budget=0.0, online=False):
         """Serve an open-loop request stream (mt_serve).  Op buffers are device
         tensors holding every request's ops; request_first_op, request_num_ops
         and arrival_ns (nanoseconds after the start, non-decreasing) are host
         arrays, one entry per request.  Returns (latency_ns numpy array, stats
-        dict).  plain=True serves one synchronous mixed_batch per request."""
+        dict).  plain=True serves one synchronous mixed_batch per request;
+        online=True takes HOST (pinned) op buffers and submits each request
+        through the online server API at its arrival time."""
         import numpy as np
         first = np.ascontiguousarray(request_first_op, dtype=np.uint32)
         nops = np.ascontiguousarray(request_num_ops, dtype=np.uint32)
@@ -217,7 +223,7 @@ class GpuMasstree:
         plan.request_num_ops = nops.ctypes.data
         plan.arrival_ns = arr.ctypes.data
         plan.num_requests = n
-        plan.mode = 1 if plain else 0
+        plan.mode = 1 if plain else (2 if online else 0)
         plan.chunk_ops, plan.epoch_us, plan.memory_budget = chunk_ops, epoch_us, memory_budget
         st = _lib.MtServeStats()
         rc = self._lib.mt_serve(self._h, ctypes.byref(plan), lat.ctypes.data, ctypes.byref(st))
@@ -227,7 +233,10 @@ class GpuMasstree:
     # -- status ---------------------------------------------------------------------
     def sync(self, stream=0):
         """Wait for the stream; raise MasstreeError if a device error was recorded."""
-        self._check(self._lib.mt_sync(self._h, _stream(stream)), "device")
+        rc = self._lib.mt_sync(self._h, _stream(stream))
+        if rc != 0:
+            site = self.stats()["device_error_site"] if rc != 5 else 0
+            raise MasstreeError(rc, "device", site)
 
     def reclaim(self, stream=0):
         self._check(self._lib.mt_reclaim(self._h, _stream(stream)), "mt_reclaim")
@@ -245,6 +254,47 @@ class GpuMasstree:
         s = _lib.MtStats()
         self._check(self._lib.mt_stats(self._h, ctypes.byref(s)), "mt_stats")
         return {f: getattr(s, f) for f, _ in _lib.MtStats._fields_}
+
+
+class MasstreeServer:
+    """Online serving of a tree (mt_server_*): submit requests from host
+    buffers while the device loop runs, poll their tickets, stop."""
+
+    def __init__(self, tree, max_key_length, max_value_length, max_ops_in_flight=0, max_requests_in_flight=0,
+                 chunk_ops=0, epoch_us=0, memory_budget=0.0):
+        self._lib = tree._lib
+        cfg = _lib.MtServerConfig(max_key_length, max_value_length, max_ops_in_flight, max_requests_in_flight,
+                                  chunk_ops, epoch_us, memory_budget, 0)
+        h = ctypes.c_void_p()
+        rc = self._lib.mt_server_start(tree._h, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise MasstreeError(rc, "mt_server_start")
+        self._h = h
+
+    def submit(self, types, keys, key_lengths, values, value_lengths, results, num_ops):
+        """Queue one request; buffers are host memory (pinned tensors or numpy
+        arrays, or integer addresses) that must stay untouched until done."""
+        t = ctypes.c_uint64()
+        rc = self._lib.mt_server_submit(self._h, _ptr(types), _ptr(keys), _ptr(key_lengths), _ptr(values),
+                                        _ptr(value_lengths), _ptr(results), num_ops, ctypes.byref(t))
+        if rc != 0:
+            raise MasstreeError(rc, "mt_server_submit")
+        return t.value
+
+    def poll(self, ticket):
+        """(done, latency_ns) of a ticket."""
+        d, lat = ctypes.c_int(), ctypes.c_uint64()
+        rc = self._lib.mt_server_poll(self._h, ticket, ctypes.byref(d), ctypes.byref(lat))
+        if rc != 0:
+            raise MasstreeError(rc, "mt_server_poll")
+        return bool(d.value), int(lat.value)
+
+    def stop(self):
+        if self._h:
+            h, self._h = self._h, None
+            rc = self._lib.mt_server_stop(h)
+            if rc != 0:
+                raise MasstreeError(rc, "mt_server_stop")
 
 
 def line_atomicity_selftest(tile_size, nlines=64, iters=20000):

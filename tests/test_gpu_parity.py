@@ -230,3 +230,37 @@ def test_empty_batches_and_pool_exhaustion():
         del z
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("depth", [40, 300])
+def test_scan_layers_beyond_scratch(tile, depth):
+    # Keys sharing `depth` - 2 leading slices build that many one-entry trie
+    # layers (suffix splits), so a scan descends deeper than the 32 layer
+    # frames held in scratch and spills the rest to slabs.
+    rng = np.random.default_rng(depth)
+    n = 24
+    maxK = depth + 1
+    keys = np.zeros((n, maxK), np.uint32)
+    keys[:, : depth - 2] = rng.integers(1, 1 << 32, depth - 2, dtype=np.uint32)
+    keys[:, depth - 2:] = rng.integers(0, 1 << 32, (n, 3), dtype=np.uint32)
+    lens = np.full(n, depth, np.uint32)
+    lens[::3] = depth + 1
+    vals = rng.integers(0, 1 << 32, (n, 2), dtype=np.uint32)
+    vlens = np.full(n, 2, np.uint32)
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        np.testing.assert_array_equal(g.insert(keys, lens, vals, vlens), o.insert(keys, lens, vals, vlens))
+        lower = np.zeros((3, maxK), np.uint32)
+        lower[1] = keys[5]
+        lower[2, : depth - 2] = keys[0, : depth - 2]
+        llen = np.array([1, lens[5], depth - 2], np.uint32)
+        a = g.scan(lower, llen, n + 4, maxV=2)
+        b = o.scan(lower, llen, n + 4, maxV=2)
+        for x, y, name in zip(a, b, ["counts", "values", "value lengths", "keys", "key lengths"]):
+            np.testing.assert_array_equal(x, y, err_msg=name)
+        assert a[0][0] == n
+        g.t.reclaim()
+        st = g.t.stats()
+        assert st["limbo_slabs"] == 0 and st["device_error"] == 0
+    finally:
+        g.close()
