@@ -583,6 +583,7 @@ def run_c1(args, stream, peak):
     1M finds (half hits, half absent keys), each timed on the device."""
     import torch
     from indexingpu_b200 import GpuMasstree
+    torch.cuda.empty_cache()  # blocks cached by earlier sections would crowd the bulk build's scratch
     d = wl.c1()
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
     k, l, v, vl = dev(d["keys"]), dev(d["lens"]), dev(d["vals"]), dev(d["vlens"])
@@ -662,6 +663,7 @@ def run_c3(args, stream, peak):
     values and lengths returned."""
     import torch
     from indexingpu_b200 import GpuMasstree
+    torch.cuda.empty_cache()
     n, nq, mc = 1 << 25, 1 << 20, 100
     d = wl.c3(n, nq)
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731

@@ -40,6 +40,7 @@ struct batch_args {
   const uint32_t* value_lengths_in;
   uint32_t* value_lengths_out;
   bool* results;
+  uint32_t* values_out;          // optional: find outputs go here instead of `values` (same row stride)
   const uint32_t* index;       // optional request subset
   const uint32_t* n_dev;       // optional device-side request count (with index)
   const uint32_t* n_back_dev;  // optional: further indices at the END of the index region
@@ -74,7 +75,8 @@ MT_DEV void run_request(const tile<T>& t, const tree_view& tv, slab_cache<T>& ca
   const uint32_t* key = a.keys + (size_t)j * a.max_key_length;
   if constexpr (op_finds<OP>) {
     if (kind == MT_REQ_FIND) {
-      uint32_t* out = a.values ? a.values + (size_t)j * a.max_value_length : nullptr;
+      uint32_t* vo = a.values_out ? a.values_out : a.values;
+      uint32_t* out = vo ? vo + (size_t)j * a.max_value_length : nullptr;
       vout = coop_find<T, CONC>(t, tv, key, klen, out, a.max_value_length);
       return;
     }

@@ -28,6 +28,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "mt_internal.cuh"
@@ -600,20 +601,18 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
 // The device loop above, fed while it runs.  Clients call mt_server_submit
 // from any host thread; the server's own host thread (the pump) moves each
 // request through: queued -> admitted (staging space, a request slot and the
-// memory budget allow; ops uploaded on the upload stream) -> published (the
-// upload finished; work items on the ring) -> downloading (the device raised
-// the slot's completion flag; results copied to the client's buffers on the
-// download stream) -> done (copies finished; mt_server_poll reports it).
-// Staging is a ring of max_ops_in_flight ops filled and freed in admission
-// order; request slots are ticket % max_requests_in_flight.
+// memory budget allow) -> uploading -> published (work items on the ring) ->
+// done.  Per pump round, the requests admitted together are copied (CPU) into
+// a pinned host staging ring and go to the device with ONE copy per field; the
+// device loop writes find values, value lengths and write results straight
+// into mapped host memory, and when the device raises a request's completion
+// flag the pump copies its results into the client's buffers and marks the
+// ticket done.  Staging is a ring of max_ops_in_flight ops, filled and freed
+// in admission order; request slots are ticket % max_requests_in_flight.
 
 namespace {
 
-__global__ void fill_u32_kernel(uint32_t* p, uint32_t v, uint32_t n) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
-}
-
-enum : uint32_t { SRV_UPLOADING = 0, SRV_PUBLISHED = 1, SRV_DOWNLOADING = 2, SRV_DONE = 3 };
+enum : uint32_t { SRV_UPLOADING = 0, SRV_PUBLISHED = 1, SRV_DONE = 2 };
 
 struct srv_request {
   uint64_t ticket = 0;
@@ -625,11 +624,15 @@ struct srv_request {
   bool* results = nullptr;
   uint32_t n = 0;
   uint64_t submit_ns = 0;
-  uint32_t off = 0;         // staging offset of the request's ops
-  uint64_t alloc_end = 0;   // staging head after its allocation
-  uint32_t demand = 0;      // slab demand estimate
+  uint32_t off = 0;        // staging offset of the request's ops
+  uint64_t alloc_end = 0;  // staging head after its allocation
+  uint32_t demand = 0;     // slab demand estimate
   uint32_t stage = SRV_UPLOADING;
-  cudaEvent_t ev = nullptr; // upload, then download
+};
+
+struct srv_round {  // requests admitted in one pump round, uploaded together
+  cudaEvent_t ev = nullptr;
+  std::vector<uint32_t> slots;
 };
 
 }  // namespace
@@ -638,11 +641,16 @@ struct mt_server {
   mt_masstree* tree = nullptr;
   mt_server_config cfg{};
   uint32_t C = 0, R = 0;
+  // Device staging of the inputs, and its pinned host mirror.
   void* dmem = nullptr;
   uint8_t* d_types = nullptr;
   uint32_t *d_keys = nullptr, *d_klens = nullptr, *d_vals = nullptr, *d_vlens = nullptr, *d_order = nullptr;
-  bool* d_results = nullptr;
-  uint32_t* h_order = nullptr;  // pinned
+  void* hmem = nullptr;
+  uint8_t* h_types = nullptr;
+  uint32_t *h_keys = nullptr, *h_klens = nullptr, *h_vals = nullptr, *h_vlens = nullptr, *h_order = nullptr;
+  // Outputs, written by the device into mapped host memory.
+  uint32_t *m_vals = nullptr, *m_vals_d = nullptr, *m_vlens = nullptr, *m_vlens_d = nullptr;
+  bool *m_results = nullptr, *m_results_d = nullptr;
   serve_item *ring = nullptr, *d_ring = nullptr;
   unsigned long long *pub = nullptr, *d_pub = nullptr;
   uint32_t *stop = nullptr, *d_stop = nullptr, *done = nullptr, *d_done = nullptr;
@@ -653,7 +661,8 @@ struct mt_server {
   server_view sv{};
   int blocks = 0;
   size_t nwarps = 0;
-  cudaStream_t s_work = nullptr, s_up = nullptr, s_down = nullptr;
+  cudaStream_t s_work = nullptr, s_up = nullptr;
+  std::vector<cudaEvent_t> ev_pool;  // pump only
   std::unique_ptr<std::atomic<uint64_t>[]> rec_ticket;
   std::unique_ptr<std::atomic<uint32_t>[]> rec_done;
   std::unique_ptr<std::atomic<uint64_t>[]> rec_latency;
@@ -674,65 +683,88 @@ namespace {
 void server_free(mt_server* S) {
   if (S->s_work) cudaStreamSynchronize(S->s_work);
   if (S->s_up) cudaStreamSynchronize(S->s_up);
-  if (S->s_down) cudaStreamSynchronize(S->s_down);
-  for (auto& r : S->slots)
-    if (r.ev) cudaEventDestroy(r.ev);
+  for (auto e : S->ev_pool) cudaEventDestroy(e);
   if (S->dmem) cudaFree(S->dmem);
-  if (S->h_order) cudaFreeHost(S->h_order);
-  for (void* h : {(void*)S->ring, (void*)S->pub, (void*)S->stop, (void*)S->done, (void*)S->usage})
+  for (void* h : {S->hmem, (void*)S->m_vals, (void*)S->m_vlens, (void*)S->m_results, (void*)S->ring,
+                  (void*)S->pub, (void*)S->stop, (void*)S->done, (void*)S->usage})
     if (h) cudaFreeHost(h);
   if (S->d_finished) cudaFree(S->d_finished);
   if (S->d_ctl) cudaFree(S->d_ctl);
   if (S->d_held) cudaFree(S->d_held);
-  for (cudaStream_t st : {S->s_work, S->s_up, S->s_down})
+  for (cudaStream_t st : {S->s_work, S->s_up})
     if (st) cudaStreamDestroy(st);
   delete S;
 }
 
-int copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind k, cudaStream_t s) {
-  if (bytes == 0) return MT_OK;
-  return cudaMemcpyAsync(dst, src, bytes, k, s) == cudaSuccess ? MT_OK : MT_ERR_CUDA;
-}
-
-// Upload request r into staging [r.off, r.off + r.n) on the upload stream.
-int server_upload(mt_server* S, srv_request& r) {
+// Copy request r's inputs into the host staging at r.off and file its ops in
+// kind order (finds, inserts, updates, erases: items cut from a request are
+// then mostly of one kind, as in mt_serve).
+void server_stage(mt_server* S, const srv_request& r) {
   const uint32_t K = S->cfg.max_key_length, V = S->cfg.max_value_length, off = r.off, n = r.n;
-  // The request's ops grouped by kind (finds, inserts, updates, erases), so
-  // that the items cut from it mostly hold one kind (as in mt_serve).
-  uint32_t pos = off;
-  for (uint8_t kind : {(uint8_t)MT_REQ_FIND, (uint8_t)MT_REQ_INSERT, (uint8_t)MT_REQ_UPDATE, (uint8_t)MT_REQ_ERASE})
-    for (uint32_t o = 0; o < n; ++o)
-      if (r.types[o] == kind) S->h_order[pos++] = off + o;
-  for (uint32_t o = 0; o < n; ++o)
-    if (r.types[o] > MT_REQ_UPDATE) S->h_order[pos++] = off + o;  // served (and reported) last
-  cudaStream_t s = S->s_up;
-  int rc = copy_async(S->d_order + off, S->h_order + off, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
-  if (!rc) rc = copy_async(S->d_types + off, r.types, n, cudaMemcpyHostToDevice, s);
-  if (!rc) rc = copy_async(S->d_keys + (size_t)off * K, r.keys, (size_t)n * K * 4u, cudaMemcpyHostToDevice, s);
-  if (!rc && r.klens) rc = copy_async(S->d_klens + off, r.klens, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
-  if (!rc && !r.klens) {
-    fill_u32_kernel<<<std::max(1u, std::min(64u, (n + 255u) / 256u)), 256, 0, s>>>(S->d_klens + off, K, n);
-    rc = cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_CUDA;
+  std::memcpy(S->h_types + off, r.types, n);
+  std::memcpy(S->h_keys + (size_t)off * K, r.keys, (size_t)n * K * 4u);
+  if (r.klens) std::memcpy(S->h_klens + off, r.klens, (size_t)n * 4u);
+  else std::fill(S->h_klens + off, S->h_klens + off + n, K);
+  std::memcpy(S->h_vals + (size_t)off * V, r.vals, (size_t)n * V * 4u);
+  std::memcpy(S->h_vlens + off, r.vlens, (size_t)n * 4u);
+  // Outputs start as the inputs: an op the device skips (invalid lengths,
+  // reported as MT_ERR_INVALID_ARG) hands its buffers back unchanged.
+  std::memcpy(S->m_vlens + off, r.vlens, (size_t)n * 4u);
+  if (r.results) std::memcpy(S->m_results + off, r.results, n);
+  uint32_t cnt[5] = {0, 0, 0, 0, 0};  // per kind rank: find, insert, update, erase, other
+  auto rank = [](uint8_t k) -> int {
+    return k == MT_REQ_FIND ? 0 : k == MT_REQ_INSERT ? 1 : k == MT_REQ_UPDATE ? 2 : k == MT_REQ_ERASE ? 3 : 4;
+  };
+  for (uint32_t o = 0; o < n; ++o) ++cnt[rank(r.types[o])];
+  uint32_t start[5];
+  uint32_t acc = off;
+  for (int k = 0; k < 5; ++k) {
+    start[k] = acc;
+    acc += cnt[k];
   }
-  if (!rc) rc = copy_async(S->d_vals + (size_t)off * V, r.vals, (size_t)n * V * 4u, cudaMemcpyHostToDevice, s);
-  if (!rc) rc = copy_async(S->d_vlens + off, r.vlens, (size_t)n * 4u, cudaMemcpyHostToDevice, s);
-  if (!rc && cudaEventRecord(r.ev, s) != cudaSuccess) rc = MT_ERR_CUDA;
-  return rc;
+  for (uint32_t o = 0; o < n; ++o) S->h_order[start[rank(r.types[o])]++] = off + o;
 }
 
-int server_download(mt_server* S, srv_request& r) {
-  const uint32_t V = S->cfg.max_value_length, off = r.off, n = r.n;
-  cudaStream_t s = S->s_down;
-  int rc = copy_async(r.vals, S->d_vals + (size_t)off * V, (size_t)n * V * 4u, cudaMemcpyDeviceToHost, s);
-  if (!rc) rc = copy_async(r.vlens, S->d_vlens + off, (size_t)n * 4u, cudaMemcpyDeviceToHost, s);
-  if (!rc && r.results) rc = copy_async(r.results, S->d_results + off, n, cudaMemcpyDeviceToHost, s);
-  if (!rc && cudaEventRecord(r.ev, s) != cudaSuccess) rc = MT_ERR_CUDA;
-  return rc;
+// Upload staging ops [lo, hi) (one contiguous run) on the upload stream.
+int server_upload_range(mt_server* S, uint32_t lo, uint32_t hi) {
+  if (hi <= lo) return MT_OK;
+  const uint32_t K = S->cfg.max_key_length, V = S->cfg.max_value_length, n = hi - lo;
+  cudaStream_t s = S->s_up;
+  auto cp = [&](void* d, const void* h, size_t bytes) {
+    return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s) == cudaSuccess;
+  };
+  const bool ok = cp(S->d_types + lo, S->h_types + lo, n) &&
+                  cp(S->d_keys + (size_t)lo * K, S->h_keys + (size_t)lo * K, (size_t)n * K * 4u) &&
+                  cp(S->d_klens + lo, S->h_klens + lo, (size_t)n * 4u) &&
+                  cp(S->d_vals + (size_t)lo * V, S->h_vals + (size_t)lo * V, (size_t)n * V * 4u) &&
+                  cp(S->d_vlens + lo, S->h_vlens + lo, (size_t)n * 4u) &&
+                  cp(S->d_order + lo, S->h_order + lo, (size_t)n * 4u);
+  return ok ? MT_OK : MT_ERR_CUDA;
+}
+
+// Results of a completed request, from the mapped outputs to its buffers:
+// find values and value lengths, write results (what mt_mixed_batch writes).
+void server_deliver(mt_server* S, const srv_request& r) {
+  const uint32_t V = S->cfg.max_value_length, off = r.off;
+  for (uint32_t o = 0; o < r.n; ++o) {
+    if (r.types[o] == MT_REQ_FIND) {
+      const uint32_t vl = S->m_vlens[off + o];
+      r.vlens[o] = vl;
+      const uint32_t c = std::min(vl, V);
+      if (c) std::memcpy(r.vals + (size_t)o * V, S->m_vals + (size_t)(off + o) * V, (size_t)c * 4u);
+    } else if (r.results && r.types[o] <= MT_REQ_UPDATE) {
+      r.results[o] = S->m_results[off + o];
+    }
+  }
 }
 
 void server_pump(mt_server* S) {
   mt_masstree* t = S->tree;
-  if (cudaSetDevice(t->device) != cudaSuccess) { S->status = MT_ERR_CUDA; return; }
+  if (cudaSetDevice(t->device) != cudaSuccess) {
+    S->status = MT_ERR_CUDA;
+    S->exited = true;
+    return;
+  }
   const uint32_t C = S->C, R = S->R;
   const uint32_t tiles_per_warp = 32u / t->tile_size;
   const uint64_t total_tiles = S->nwarps * tiles_per_warp;
@@ -741,19 +773,31 @@ void server_pump(mt_server* S) {
   const double budget = S->cfg.memory_budget > 0.f ? S->cfg.memory_budget : 0.9;
   const unsigned long long epoch_ns = (unsigned long long)(S->cfg.epoch_us ? S->cfg.epoch_us : 20000u) * 1000ull;
   const uint32_t per_write = 1u + suf_nodes(S->cfg.max_key_length, S->cfg.max_value_length);
+  int rc = MT_OK;
   mt_stats_t st{};
-  if (mt_stats(t, &st) != MT_OK) { S->status = MT_ERR_CUDA; return; }
+  if (mt_stats(t, &st) != MT_OK) rc = MT_ERR_CUDA;
   const double slab_budget = budget * (double)st.total_slabs;
   double slabs_in_use = (double)st.used_slabs + (double)st.limbo_slabs;
   uint64_t admitted_demand = 0, completed_demand = 0;
 
-  std::deque<uint32_t> fifo, upq, downq;  // slots, in admission / upload / download order
-  std::vector<uint32_t> published;        // slots waiting for the device
-  uint64_t head = 0, tail = 0;            // staging ring (ops)
+  std::deque<uint32_t> fifo;      // slots in admission order (frees staging)
+  std::deque<srv_round> rounds;   // upload rounds in flight, in order
+  std::vector<uint32_t> published;
+  uint64_t head = 0, tail = 0;    // staging ring (ops)
   uint64_t items_published = 0, admitted_ops = 0, completed_ops = 0;
   std::vector<cudaEvent_t> evs;
   std::vector<uint64_t> enq_completed;
   size_t ev_done = 0;
+  auto take_event = [&]() -> cudaEvent_t {
+    if (!S->ev_pool.empty()) {
+      cudaEvent_t e = S->ev_pool.back();
+      S->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    return e;
+  };
   auto enqueue_epoch = [&]() -> int {
     int r2 = host_launch_reclaim(t, S->s_work);
     if (r2) return r2;
@@ -767,13 +811,16 @@ void server_pump(mt_server* S) {
     enq_completed.push_back(completed_demand);
     return MT_OK;
   };
-  int rc = enqueue_epoch();
+  if (!rc) rc = enqueue_epoch();
   if (!rc) rc = enqueue_epoch();
   uint64_t stuck_since = 0;
   while (!rc) {
     bool progress = false;
-    // ---- admit queued requests in order --------------------------------------
-    while (true) {
+    // ---- admit queued requests in order, staged and uploaded together ------
+    srv_round round;
+    uint32_t run_lo = 0, run_hi = 0;  // current contiguous staging run
+    bool have_run = false;
+    while (!rc) {
       srv_request r;
       {
         std::lock_guard<std::mutex> g(S->mu);
@@ -805,56 +852,73 @@ void server_pump(mt_server* S) {
         r.demand = d;
       }
       const uint32_t slot = (uint32_t)(r.ticket % R);
-      srv_request& q = S->slots[slot];
-      r.ev = q.ev;
       r.stage = SRV_UPLOADING;
-      q = r;
+      S->slots[slot] = r;
       S->rec_done[slot].store(0u, std::memory_order_relaxed);
       S->rec_ticket[slot].store(r.ticket, std::memory_order_release);
       slabs_in_use += r.demand;
       admitted_demand += r.demand;
       admitted_ops += r.n;
-      rc = server_upload(S, q);
-      if (rc) break;
+      server_stage(S, r);
+      if (have_run && r.off == run_hi) {
+        run_hi += r.n;
+      } else {
+        if (have_run) rc = server_upload_range(S, run_lo, run_hi);
+        run_lo = r.off;
+        run_hi = r.off + r.n;
+        have_run = true;
+      }
       fifo.push_back(slot);
-      upq.push_back(slot);
+      round.slots.push_back(slot);
       progress = true;
     }
-    // ---- publish uploaded requests as work items -------------------------------
-    while (!rc && !upq.empty() && cudaEventQuery(S->slots[upq.front()].ev) == cudaSuccess) {
-      const uint32_t slot = upq.front();
-      upq.pop_front();
-      srv_request& q = S->slots[slot];
-      uint32_t chunk = fixed_chunk;
-      if (auto_chunk) {
-        const uint64_t backlog = admitted_ops - std::min(admitted_ops, completed_ops);
-        const uint64_t per_tile = backlog / total_tiles;
-        chunk = backlog < S->nwarps / 8 ? 1u
-                                         : tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
-      }
-      const uint32_t n_items = std::max<uint32_t>(1u, (q.n + chunk - 1) / chunk);
-      S->done[slot] = 0u;
-      uint32_t f = q.off, left = q.n;
-      for (uint32_t k = 0; k < n_items; ++k) {
-        const uint32_t c = std::min(left, chunk);
-        S->ring[items_published % C] = serve_item{slot, f, c, n_items};
-        ++items_published;
-        f += c;
-        left -= c;
+    if (!rc && have_run) {
+      rc = server_upload_range(S, run_lo, run_hi);
+      round.ev = take_event();
+      if (!round.ev || cudaEventRecord(round.ev, S->s_up) != cudaSuccess) rc = MT_ERR_CUDA;
+      if (!rc) rounds.push_back(std::move(round));
+    }
+    // ---- publish uploaded rounds as work items --------------------------------
+    while (!rc && !rounds.empty() && cudaEventQuery(rounds.front().ev) == cudaSuccess) {
+      srv_round& rd = rounds.front();
+      for (uint32_t slot : rd.slots) {
+        srv_request& q = S->slots[slot];
+        uint32_t chunk = fixed_chunk;
+        if (auto_chunk) {
+          const uint64_t backlog = admitted_ops - std::min(admitted_ops, completed_ops);
+          const uint64_t per_tile = backlog / total_tiles;
+          chunk = backlog < S->nwarps / 8 ? 1u
+                                           : tiles_per_warp * (per_tile < 1 ? 1u : per_tile < 2 ? 2u : per_tile < 4 ? 4u : 8u);
+        }
+        const uint32_t n_items = std::max<uint32_t>(1u, (q.n + chunk - 1) / chunk);
+        S->done[slot] = 0u;
+        uint32_t f = q.off, left = q.n;
+        for (uint32_t k = 0; k < n_items; ++k) {
+          const uint32_t c = std::min(left, chunk);
+          S->ring[items_published % C] = serve_item{slot, f, c, n_items};
+          ++items_published;
+          f += c;
+          left -= c;
+        }
+        q.stage = SRV_PUBLISHED;
+        published.push_back(slot);
       }
       __atomic_store_n(S->pub, (unsigned long long)items_published, __ATOMIC_RELEASE);
-      q.stage = SRV_PUBLISHED;
-      published.push_back(slot);
+      S->ev_pool.push_back(rd.ev);
+      rounds.pop_front();
       progress = true;
     }
-    // ---- completed on the device: download the results --------------------------
+    // ---- completed on the device: deliver the results -------------------------
     for (size_t k = 0; !rc && k < published.size();) {
       const uint32_t slot = published[k];
       if (__atomic_load_n(&S->done[slot], __ATOMIC_ACQUIRE)) {
         srv_request& q = S->slots[slot];
-        rc = server_download(S, q);
-        q.stage = SRV_DOWNLOADING;
-        downq.push_back(slot);
+        server_deliver(S, q);
+        q.stage = SRV_DONE;
+        completed_demand += q.demand;
+        completed_ops += q.n;
+        S->rec_latency[slot].store(now_ns(S->t0) - q.submit_ns, std::memory_order_relaxed);
+        S->rec_done[slot].store(1u, std::memory_order_release);
         published[k] = published.back();
         published.pop_back();
         progress = true;
@@ -862,20 +926,8 @@ void server_pump(mt_server* S) {
         ++k;
       }
     }
-    // ---- downloads finished: the tickets are done -------------------------------
-    while (!rc && !downq.empty() && cudaEventQuery(S->slots[downq.front()].ev) == cudaSuccess) {
-      const uint32_t slot = downq.front();
-      downq.pop_front();
-      srv_request& q = S->slots[slot];
-      q.stage = SRV_DONE;
-      completed_demand += q.demand;
-      completed_ops += q.n;
-      S->rec_latency[slot].store(now_ns(S->t0) - q.submit_ns, std::memory_order_relaxed);
-      S->rec_done[slot].store(1u, std::memory_order_release);
-      progress = true;
-    }
     while (!fifo.empty() && S->slots[fifo.front()].stage == SRV_DONE) {
-      tail = S->slots[fifo.front()].alloc_end > tail ? S->slots[fifo.front()].alloc_end : tail;
+      tail = std::max(tail, S->slots[fifo.front()].alloc_end);
       fifo.pop_front();
     }
     // ---- keep the device loop running -------------------------------------------
@@ -905,7 +957,7 @@ void server_pump(mt_server* S) {
   __atomic_store_n(S->stop, 1u, __ATOMIC_RELEASE);
   cudaStreamSynchronize(S->s_work);
   cudaStreamSynchronize(S->s_up);
-  cudaStreamSynchronize(S->s_down);
+  for (auto& rd : rounds) S->ev_pool.push_back(rd.ev);
   for (auto e : evs) cudaEventDestroy(e);
   if (rc) S->status = rc;
   S->exited.store(true, std::memory_order_release);
@@ -925,26 +977,34 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
   S->R = cfg->max_requests_in_flight ? cfg->max_requests_in_flight : 65536u;
   const uint32_t C = S->C, R = S->R, K = cfg->max_key_length, V = cfg->max_value_length;
   auto up = [](size_t b) { return (b + 255u) & ~size_t(255); };
-  const size_t bytes = up(C) + up((size_t)C * K * 4u) + 3 * up((size_t)C * 4u) + up((size_t)C * V * 4u) + up(C);
-  bool ok = cudaMalloc(&S->dmem, bytes) == cudaSuccess;
+  const size_t bytes = up(C) + up((size_t)C * K * 4u) + 3 * up((size_t)C * 4u) + up((size_t)C * V * 4u);
+  bool ok = cudaMalloc(&S->dmem, bytes) == cudaSuccess && cudaMallocHost(&S->hmem, bytes) == cudaSuccess;
   if (ok) {
     char* p = static_cast<char*>(S->dmem);
-    S->d_types = reinterpret_cast<uint8_t*>(p); p += up(C);
-    S->d_keys = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * K * 4u);
-    S->d_klens = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
-    S->d_vlens = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
-    S->d_order = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * 4u);
-    S->d_vals = reinterpret_cast<uint32_t*>(p); p += up((size_t)C * V * 4u);
-    S->d_results = reinterpret_cast<bool*>(p);
+    char* h = static_cast<char*>(S->hmem);
+    auto carve = [&](size_t b, auto** dptr, auto** hptr) {
+      *dptr = reinterpret_cast<std::remove_pointer_t<decltype(dptr)>>(p);
+      *hptr = reinterpret_cast<std::remove_pointer_t<decltype(hptr)>>(h);
+      p += up(b);
+      h += up(b);
+    };
+    carve(C, &S->d_types, &S->h_types);
+    carve((size_t)C * K * 4u, &S->d_keys, &S->h_keys);
+    carve((size_t)C * 4u, &S->d_klens, &S->h_klens);
+    carve((size_t)C * 4u, &S->d_vlens, &S->h_vlens);
+    carve((size_t)C * 4u, &S->d_order, &S->h_order);
+    carve((size_t)C * V * 4u, &S->d_vals, &S->h_vals);
   }
-  ok = ok && cudaMallocHost(&S->h_order, (size_t)C * 4u) == cudaSuccess;
   if (ok) {
+    S->m_vals = mapped_alloc<uint32_t>((size_t)C * V, &S->m_vals_d);
+    S->m_vlens = mapped_alloc<uint32_t>(C, &S->m_vlens_d);
+    S->m_results = mapped_alloc<bool>(C, &S->m_results_d);
     S->ring = mapped_alloc<serve_item>(C, &S->d_ring);
     S->pub = mapped_alloc<unsigned long long>(1, &S->d_pub);
     S->stop = mapped_alloc<uint32_t>(1, &S->d_stop);
     S->done = mapped_alloc<uint32_t>(R, &S->d_done);
     S->usage = mapped_alloc<unsigned long long>(1, &S->d_usage);
-    ok = S->ring && S->pub && S->stop && S->done && S->usage;
+    ok = S->m_vals && S->m_vlens && S->m_results && S->ring && S->pub && S->stop && S->done && S->usage;
   }
   S->blocks = server_blocks_tile(t);
   S->nwarps = (size_t)S->blocks * (kBlock / 32);
@@ -955,15 +1015,13 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
        cudaMalloc(&S->d_held, S->nwarps * sizeof(unsigned long long)) == cudaSuccess &&
        cudaMemset(S->d_held, 0xFF, S->nwarps * sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&S->s_work, cudaStreamNonBlocking) == cudaSuccess &&
-       cudaStreamCreateWithFlags(&S->s_up, cudaStreamNonBlocking) == cudaSuccess &&
-       cudaStreamCreateWithFlags(&S->s_down, cudaStreamNonBlocking) == cudaSuccess;
+       cudaStreamCreateWithFlags(&S->s_up, cudaStreamNonBlocking) == cudaSuccess;
   if (ok) {
     S->slots.resize(R);
-    for (auto& r : S->slots) ok = ok && cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming) == cudaSuccess;
     S->rec_ticket.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
     S->rec_done.reset(new (std::nothrow) std::atomic<uint32_t>[R]);
     S->rec_latency.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
-    ok = ok && S->rec_ticket && S->rec_done && S->rec_latency;
+    ok = S->rec_ticket && S->rec_done && S->rec_latency;
     for (uint32_t k = 0; ok && k < R; ++k) {
       S->rec_ticket[k].store(0);
       S->rec_done[k].store(0);
@@ -988,10 +1046,11 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
   ops.types = S->d_types;
   ops.keys = S->d_keys;
   ops.key_lengths = S->d_klens;
-  ops.values = S->d_vals;
+  ops.values = S->d_vals;            // insert and update values
+  ops.values_out = S->m_vals_d;      // find values, to mapped host memory
   ops.value_lengths_in = S->d_vlens;
-  ops.value_lengths_out = S->d_vlens;
-  ops.results = S->d_results;
+  ops.value_lengths_out = S->m_vlens_d;
+  ops.results = S->m_results_d;
   ops.max_key_length = K;
   ops.max_value_length = V;
   sv.ops = ops;
