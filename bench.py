@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=1 << 20)
     ap.add_argument("--tile", type=int, default=8, help="lanes per find")
     ap.add_argument("--write-tile", type=int, default=32, help="lanes per insert/update/erase")
+    ap.add_argument("--upderase-tile", type=int, default=0,
+                    help="lanes per update/erase of a mixed batch (0: the write width)")
     ap.add_argument("--scan-tile", type=int, default=4, help="lanes per scan query (c3 section)")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--bucket", type=int, default=0, help="1: mixed_batch serves short keys before long keys")
@@ -237,6 +239,7 @@ def run_ours(args, rank, world, dist):
     else:
         tree = GpuMasstree(pool_ratio=0.6, tile_size=args.tile)
     tree.set_write_tile_size(args.write_tile)
+    tree.set_upderase_tile_size(args.upderase_tile)
     if args.blocks_per_sm:
         tree.set_blocks_per_sm(args.blocks_per_sm)
     stream = torch.cuda.current_stream()
@@ -371,6 +374,7 @@ def run_ours(args, rank, world, dist):
                                    "after a 16M-key preload; keys 2-16 slices, 4096 shared prefixes; values 1-8 slices",
                        "preload_keys": args.preload, "batch_requests": args.batch, "max_key_length": MAXK,
                        "max_value_length": MAXV, "tile_size": args.tile, "write_tile_size": args.write_tile,
+                       "upderase_tile_size": args.upderase_tile or args.write_tile,
                        "form": "plain per-call mixed_batch (reclaim, three-way partition, find / insert / "
                                "update+erase class kernels on forked streams)",
                        "l2": "no flush: the index (>2 GB of slabs) and each batch's inputs exceed the 126 MB L2",

@@ -58,6 +58,9 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
                                        nodes left with 4 entries or fewer into a neighbour under
                                        the same parent (reference erase merge levels 2-4; space
                                        only, results are the same) */
+#define MT_FLAG_INPUTS_ON_STREAM 256u /* mixed_batch_host: the uploads wait for the work queued on `stream`
+                                       before the call (for host inputs that work produces, e.g. a copy
+                                       queued just before); without it the uploads start at once */
 #define MT_FLAG_REMOVE_EMPTY_LAYERS 128u /* erase, mixed_batch: after the call's erases (and merges),
                                        remove every trie layer (1 or deeper, reached by at most 15
                                        key slices) whose only node they left empty, and the parent
@@ -109,6 +112,11 @@ int mt_set_tile_size(mt_masstree* tree, uint32_t tile_size);
  * sets both widths). */
 int mt_set_write_tile_size(mt_masstree* tree, uint32_t tile_size);
 int mt_set_blocks_per_sm(mt_masstree* tree, uint32_t blocks_per_sm);
+/* Lanes per update or erase request of mixed batches (4/8/16/32; 0 = the
+ * write width, the default).  Under skewed key choice most of them miss (the
+ * key was erased) and end in a lock-free check, which narrow tiles serve many
+ * at a time.  New in this library. */
+int mt_set_upderase_tile_size(mt_masstree* tree, uint32_t tile_size);
 /* Lanes per scan query (4/8/16/32; 0 = the find width, the default).  Scans
  * read many independent suffix lines per query and run fastest with narrow
  * tiles (more queries in flight).  New in this library. */
@@ -181,7 +189,9 @@ int mt_mixed_batch(mt_masstree* tree, const uint8_t* request_types, const uint32
  * mt_mixed_batch (one of the orders a mixed batch allows).  Asynchronous:
  * the input buffers are read from the moment of the call on (they must hold
  * the requests then, and the uploads do not wait for earlier work on
- * `stream`), the work and the results are ordered on `stream`, and all host
+ * `stream`, unless flags hold MT_FLAG_INPUTS_ON_STREAM, which makes them wait
+ * for it at the cost of the overlap with the previous call's work), the work
+ * and the results are ordered on `stream`, and all host
  * buffers must stay untouched until the stream reaches the end of the call
  * (results are in host memory then).  The first call, and a
  * call with longer rows or larger chunks than before, allocates the staging

@@ -20,6 +20,7 @@ SIGNATURES = {
     "mt_set_blocks_per_sm": (_int, [_p, _u32]),
     "mt_set_scan_tile_size": (_int, [_p, _u32]),
     "mt_set_lock_wait": (_int, [_p, _u32]),
+    "mt_set_upderase_tile_size": (_int, [_p, _u32]),
     "mt_inject_node_lock": (_int, [_p, _u32, _int]),
     "mt_find": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _u32, _p]),
     "mt_insert": (_int, [_p, _p, _u32, _p, _p, _u32, _p, _u32, _p, _u32, _p]),

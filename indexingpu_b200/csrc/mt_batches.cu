@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_persiste
 // One class of one sub-batch (the forked form): the class kernels of a
 // sub-batch run side by side, each compiled for its class only.
 template <int T, int OP>
-__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batches_class_kernel(tree_view tv, batches_view b,
+__global__ void __launch_bounds__(kBlock, min_blocks_for<OP>) batches_class_kernel(tree_view tv, batches_view b,
                                                                                      uint32_t sb) {
   if (b.status[0]) return;
   constexpr uint32_t cls = OP == OP_FIND ? 0u : (OP == OP_PASS_INSERT ? 1u : 2u);
@@ -206,12 +206,13 @@ int launch_class_tile(mt_masstree* t, uint32_t tile, const batches_view& b, uint
 // the next sub-batch starts.
 int launch_forked(mt_masstree* t, const batches_view& b, cudaStream_t s) {
   const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
+  const uint32_t tu = t->upderase_tile_size ? t->upderase_tile_size : tw;
   for (uint32_t sb = 0; sb < b.nsub; ++sb) {
     int rc = host_fork(t, s);
     if (rc) return rc;
     rc = launch_class_tile<OP_PASS_INSERT>(t, tw, b, sb, s);
     if (!rc) rc = launch_class_tile<OP_FIND>(t, t->tile_size, b, sb, t->side[0]);
-    if (!rc) rc = launch_class_tile<OP_PASS_UPDERASE>(t, tw, b, sb, t->side[1]);
+    if (!rc) rc = launch_class_tile<OP_PASS_UPDERASE>(t, tu, b, sb, t->side[1]);
     rc = host_join(t, s, rc);
     if (rc) return rc;
   }

@@ -89,7 +89,7 @@ __global__ void partition3_kernel(const uint8_t* types, const uint32_t* key_leng
 }
 
 template <int T, int OP, bool CONC>
-__global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) batch_kernel(tree_view tv, batch_args a) {
+__global__ void __launch_bounds__(kBlock, min_blocks_for<OP>) batch_kernel(tree_view tv, batch_args a) {
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
@@ -370,9 +370,10 @@ int launch_mixed_split(mt_masstree* t, batch_args a, bool bucket_keys, cudaStrea
   // Write classes run with 16- or 32-lane tiles (narrower write tiles, allowed
   // for plain insert/update/erase calls, are widened to 16 here).
   const uint32_t tw = t->write_tile_size <= 16 ? 16u : 32u;
+  const uint32_t tu = t->upderase_tile_size ? t->upderase_tile_size : tw;
   rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
   if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
-  if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tw, u, t->side[1]);
+  if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tu, u, t->side[1]);
   return host_join(t, s, rc);
 }
 
@@ -554,6 +555,12 @@ int mt_inject_node_lock(mt_masstree* t, uint32_t slab, int locked) {
   // The LOCK bit is outside the node checksum, so the image stays valid.
   meta = locked ? (meta | META_LOCK) : (meta & ~META_LOCK);
   return cuda_status(cudaMemcpy(mw, &meta, sizeof(meta), cudaMemcpyHostToDevice));
+}
+
+int mt_set_upderase_tile_size(mt_masstree* t, uint32_t ts) {
+  if (!t || (ts != 0 && !valid_tile(ts))) return MT_ERR_INVALID_ARG;
+  t->upderase_tile_size = ts;
+  return MT_OK;
 }
 
 int mt_set_blocks_per_sm(mt_masstree* t, uint32_t b) {

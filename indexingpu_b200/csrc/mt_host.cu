@@ -40,6 +40,7 @@ struct mt_host_pipe {
   void* mem = nullptr;
   uint32_t chunk = 0, max_k = 0, max_v = 0;
   cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t inputs_ready = nullptr;  // MT_FLAG_INPUTS_ON_STREAM: the caller's stream reached the call
   host_slot slot[kSlots];
   uint64_t next = 0;  // chunks issued so far (slot = next % kSlots)
 };
@@ -55,6 +56,7 @@ void host_pipe_free(mt_masstree* t) {
     if (s.served) cudaEventDestroy(s.served);
     if (s.downloaded) cudaEventDestroy(s.downloaded);
   }
+  if (hp->inputs_ready) cudaEventDestroy(hp->inputs_ready);
   if (hp->up) cudaStreamDestroy(hp->up);
   if (hp->down) cudaStreamDestroy(hp->down);
   delete hp;
@@ -93,7 +95,8 @@ int ensure_pipe(mt_masstree* t, uint32_t chunk, uint32_t max_k, uint32_t max_v) 
   hp->max_v = max_v;
   char* p = static_cast<char*>(hp->mem);
   bool ok = cudaStreamCreateWithFlags(&hp->up, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&hp->down, cudaStreamNonBlocking) == cudaSuccess;
+            cudaStreamCreateWithFlags(&hp->down, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&hp->inputs_ready, cudaEventDisableTiming) == cudaSuccess;
   for (auto& s : hp->slot) {
     s.types = reinterpret_cast<uint8_t*>(p);
     p += up16(c);
@@ -136,6 +139,13 @@ extern "C" int mt_mixed_batch_host(mt_masstree* t, const uint8_t* types, const u
   int rc = ensure_pipe(t, chunk, maxK, maxV);
   if (rc) return rc;
   mt_host_pipe* hp = t->host_pipe;
+  if (flags & MT_FLAG_INPUTS_ON_STREAM) {
+    // The inputs are produced by work already queued on the caller's stream.
+    if (cudaEventRecord(hp->inputs_ready, s) != cudaSuccess ||
+        cudaStreamWaitEvent(hp->up, hp->inputs_ready, 0) != cudaSuccess)
+      return MT_ERR_CUDA;
+  }
+  flags &= ~MT_FLAG_INPUTS_ON_STREAM;
   // Rows keep the caller's strides inside a slot (its rows are at least as long).
   for (uint32_t first = 0; first < n; first += chunk) {
     const uint32_t m = std::min(chunk, n - first);

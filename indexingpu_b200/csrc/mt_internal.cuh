@@ -19,6 +19,9 @@ constexpr uint32_t kClassBarrierMin = 1u << 17;
 #ifndef MT_MIN_BLOCKS_PER_SM
 #define MT_MIN_BLOCKS_PER_SM 8  // occupancy hint for the batch kernels: caps registers at 64
 #endif
+#ifndef MT_WRITE_MIN_BLOCKS_PER_SM
+#define MT_WRITE_MIN_BLOCKS_PER_SM MT_MIN_BLOCKS_PER_SM  // the same for kernels that insert
+#endif
 
 // Kernel flavours.  OP_PASS_* serve one class of a partitioned mixed batch and
 // compile only that class's code (smaller kernels, fewer instruction-cache
@@ -28,6 +31,9 @@ enum op_kind : int {
   OP_PASS_INSERT = 6, OP_PASS_UPDERASE = 7
 };
 template <int OP> constexpr bool op_finds = OP == OP_FIND || OP == OP_MIXED;
+// Occupancy hint of a batch kernel of kind OP.
+template <int OP> constexpr int min_blocks_for =
+    (OP == OP_INSERT || OP == OP_UPSERT || OP == OP_PASS_INSERT) ? MT_WRITE_MIN_BLOCKS_PER_SM : MT_MIN_BLOCKS_PER_SM;
 template <int OP> constexpr bool op_inserts = OP == OP_INSERT || OP == OP_UPSERT || OP == OP_MIXED || OP == OP_PASS_INSERT;
 template <int OP> constexpr bool op_updates = OP == OP_UPDATE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
 template <int OP> constexpr bool op_erases = OP == OP_ERASE || OP == OP_MIXED || OP == OP_PASS_UPDERASE;
@@ -171,6 +177,7 @@ struct mt_masstree {
   int sms = 0;
   uint32_t tile_size = 8;        // finds and scans
   uint32_t write_tile_size = 8;  // inserts, updates, erases
+  uint32_t upderase_tile_size = 0;  // updates and erases of mixed batches (0: the write width)
   uint32_t scan_tile_size = 0;   // scans (0: the find width)
   uint32_t blocks_per_sm = 0;    // 0 = occupancy limit
   uint32_t* split_idx = nullptr; // mixed-batch partition scratch

@@ -35,6 +35,10 @@ namespace mtb {
 constexpr uint32_t kMaxHops = 1u << 16;     // node visits per operation
 constexpr uint32_t kLockSpins = 1u << 20;   // default lock attempts (about 1 s) before MT_ERR_LOCK_TIMEOUT
 constexpr uint32_t kMaxRestarts = 1u << 14;
+#ifndef MT_LOCK_POLLS
+#define MT_LOCK_POLLS 0
+#endif
+constexpr uint32_t kLockPolls = MT_LOCK_POLLS;  // lock retries without a sleep before the backoff starts
 
 #ifndef MT_CONC_LOAD
 #define MT_CONC_LOAD ::mtb::ld_order::RELAXED
@@ -106,9 +110,13 @@ MT_DEV bool lock_load(const tile<T>& t, const pool_view& p, uint32_t idx, node<T
       return nd.template load_verified<ld_order::ACQUIRE>(t, p, idx) || (unlock_node(t, p, idx), false);
     }
     if ((it & 255u) == 255u && t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) return false;
-    jitter = jitter * 1664525u + 1013904223u;
-    __nanosleep(backoff + ((jitter >> 16) & (backoff - 1u)));
-    if (backoff < 512u) backoff <<= 1;
+    // The first retries poll (a holder usually releases within a few hundred
+    // nanoseconds); later ones sleep with jittered exponential backoff.
+    if (it + 1u > kLockPolls) {
+      jitter = jitter * 1664525u + 1013904223u;
+      __nanosleep(backoff + ((jitter >> 16) & (backoff - 1u)));
+      if (backoff < 512u) backoff <<= 1;
+    }
   }
   if (t.leader()) record_error(p, ERR_LOCK_TIMEOUT, MT_AT(SRC_TREE));
   return false;

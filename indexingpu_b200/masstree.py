@@ -30,6 +30,7 @@ FLAG_CONCURRENT, FLAG_UPDATE_IF_EXISTS, FLAG_USE_UPPER_KEY, FLAG_SINGLE_PASS, FL
 FLAG_PERSISTENT = 32
 FLAG_MERGE = 64
 FLAG_REMOVE_EMPTY_LAYERS = 128
+FLAG_INPUTS_ON_STREAM = 256
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
@@ -110,6 +111,10 @@ class GpuMasstree:
     def set_blocks_per_sm(self, blocks_per_sm):
         self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
 
+    def set_upderase_tile_size(self, tile_size):
+        """Lanes per update/erase of mixed batches (0: the write width)."""
+        self._check(self._lib.mt_set_upderase_tile_size(self._h, tile_size), "mt_set_upderase_tile_size")
+
     def set_lock_wait(self, attempts):
         """Lock attempts before a waiting request reports MT_ERR_LOCK_TIMEOUT."""
         self._check(self._lib.mt_set_lock_wait(self._h, attempts), "mt_set_lock_wait")
@@ -171,14 +176,16 @@ class GpuMasstree:
         self._check(rc, "mt_mixed_batch")
 
     def mixed_batch_host(self, request_types, keys, max_key_length, key_lengths, values, max_value_length,
-                         value_lengths, results, num_requests, stream=0, chunk=0, bucket_keys=False):
+                         value_lengths, results, num_requests, stream=0, chunk=0, bucket_keys=False,
+                         inputs_on_stream=False):
         """mixed_batch with every buffer in (pinned) host memory; uploads, work and
         downloads of consecutive chunks overlap.  Asynchronous: sync(stream)
-        before reading the results or reusing the buffers."""
+        before reading the results or reusing the buffers.  inputs_on_stream:
+        the uploads wait for work already queued on `stream` (inputs it writes)."""
+        flags = (FLAG_BUCKET_KEYS if bucket_keys else 0) | (FLAG_INPUTS_ON_STREAM if inputs_on_stream else 0)
         rc = self._lib.mt_mixed_batch_host(self._h, _ptr(request_types), _ptr(keys), max_key_length,
                                            _ptr(key_lengths), _ptr(values), max_value_length, _ptr(value_lengths),
-                                           _ptr(results), num_requests, chunk,
-                                           FLAG_BUCKET_KEYS if bucket_keys else 0, _stream(stream))
+                                           _ptr(results), num_requests, chunk, flags, _stream(stream))
         self._check(rc, "mt_mixed_batch_host")
 
     # -- many sub-batches in one call ------------------------------------------------

@@ -121,3 +121,32 @@ def test_host_batch_without_lengths_or_results():
     finally:
         ref.close()
         new.close()
+
+
+def test_host_batch_inputs_written_by_the_stream():
+    """MT_FLAG_INPUTS_ON_STREAM: the host inputs are filled by copies queued on
+    the same stream just before the call (from device tensors); the uploads
+    must wait for them."""
+    import torch
+    c2 = wl.C2(n_preload=N_PRE, n_prefixes=64)
+    ref, new = _trees(torch, c2)
+    try:
+        bt = _touch_once(c2.batch(11, 6000))
+        exp = _device_call(torch, ref, bt)
+        n = len(bt["types"])
+        src = {k: torch.from_numpy(np.ascontiguousarray(bt[k])).cuda() for k in ("types", "keys", "lens", "vals",
+                                                                              "vlens")}
+        h = {k: torch.zeros_like(src[k], device="cpu").pin_memory() for k in src}
+        res = torch.zeros(n, dtype=torch.bool).pin_memory()
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            torch.cuda._sleep(2_000_000)  # the copies below land well after the call is made
+            for k in src:
+                h[k].copy_(src[k], non_blocking=True)
+        new.mixed_batch_host(h["types"], h["keys"], MAXK, h["lens"], h["vals"], MAXV, h["vlens"], res, n, stream=s,
+                             inputs_on_stream=True)
+        new.sync(s)
+        _check(bt, (h["vals"].numpy(), h["vlens"].numpy(), res.numpy()), exp)
+    finally:
+        ref.close()
+        new.close()
