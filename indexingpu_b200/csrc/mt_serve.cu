@@ -23,6 +23,8 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -635,6 +637,88 @@ struct srv_round {  // requests admitted in one pump round, uploaded together
   std::vector<uint32_t> slots;
 };
 
+// A few host threads that help the pump copy requests in and results out
+// (one host core moving about 100 bytes per op in and out caps the server
+// far below the device loop).  run(n, f) calls f(0..n-1) on the pool and the
+// caller and returns when all calls have ended and no worker is in the loop.
+struct copy_pool {
+  std::vector<std::thread> th;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::function<void(size_t)> fn;
+  size_t n = 0;
+  uint64_t gen = 0;
+  bool stop = false;
+  std::atomic<size_t> next{0}, finished{0};
+  std::atomic<int> active{0};
+  std::atomic<uint64_t> gen_seen{0};  // gen, readable without the lock (polling workers)
+  std::atomic<bool> stop_seen{false};
+
+  void start(int workers) {
+    for (int k = 0; k < workers; ++k) th.emplace_back([this] { loop(); });
+  }
+  void loop() {
+    uint64_t seen = 0;
+    while (true) {
+      // Poll for new work for a while (a sleeping worker takes tens of
+      // microseconds to wake), then sleep until notified.
+      for (int spin = 0; spin < 20000 && gen_seen.load(std::memory_order_acquire) == seen &&
+                         !stop_seen.load(std::memory_order_acquire);
+           ++spin)
+        std::this_thread::yield();
+      std::function<void(size_t)> f;
+      size_t cnt = 0;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop || gen != seen; });
+        if (stop) return;
+        seen = gen;
+        f = fn;
+        cnt = n;
+        active.fetch_add(1);
+      }
+      for (size_t k; (k = next.fetch_add(1)) < cnt;) {
+        f(k);
+        finished.fetch_add(1);
+      }
+      active.fetch_sub(1);
+    }
+  }
+  void run(size_t cnt, const std::function<void(size_t)>& f) {
+    if (th.empty() || cnt < 2) {
+      for (size_t k = 0; k < cnt; ++k) f(k);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> g(mu);
+      fn = f;
+      n = cnt;
+      next = 0;
+      finished = 0;
+      ++gen;
+      gen_seen.store(gen, std::memory_order_release);
+    }
+    cv.notify_all();
+    for (size_t k; (k = next.fetch_add(1)) < cnt;) {
+      f(k);
+      finished.fetch_add(1);
+    }
+    while (finished.load() < cnt || active.load() != 0) std::this_thread::yield();
+  }
+  ~copy_pool() {
+    {
+      std::lock_guard<std::mutex> g(mu);
+      stop = true;
+      stop_seen.store(true, std::memory_order_release);
+    }
+    cv.notify_all();
+    for (auto& x : th) x.join();
+  }
+};
+
+constexpr uint64_t kPoolMinOps = 4096;     // rounds this large are copied by the pool
+constexpr uint64_t kRoundMaxOps = 1u << 17;  // a round admits at most this many ops (then uploads)
+
 }  // namespace
 
 struct mt_server {
@@ -667,6 +751,7 @@ struct mt_server {
   std::unique_ptr<std::atomic<uint32_t>[]> rec_done;
   std::unique_ptr<std::atomic<uint64_t>[]> rec_latency;
   std::vector<srv_request> slots;  // pump thread only
+  copy_pool pool;                  // helps the pump copy (pump thread only)
   std::mutex mu;
   std::deque<srv_request> queued;  // under mu
   std::atomic<uint64_t> next_ticket{0};
@@ -782,7 +867,7 @@ void server_pump(mt_server* S) {
 
   std::deque<uint32_t> fifo;      // slots in admission order (frees staging)
   std::deque<srv_round> rounds;   // upload rounds in flight, in order
-  std::vector<uint32_t> published;
+  std::vector<uint32_t> published, finished_now;
   uint64_t head = 0, tail = 0;    // staging ring (ops)
   uint64_t items_published = 0, admitted_ops = 0, completed_ops = 0;
   std::vector<cudaEvent_t> evs;
@@ -818,13 +903,14 @@ void server_pump(mt_server* S) {
     bool progress = false;
     // ---- admit queued requests in order, staged and uploaded together ------
     srv_round round;
+    uint64_t round_ops = 0;
     uint32_t run_lo = 0, run_hi = 0;  // current contiguous staging run
     bool have_run = false;
     while (!rc) {
       srv_request r;
       {
         std::lock_guard<std::mutex> g(S->mu);
-        if (S->queued.empty()) break;
+        if (S->queued.empty() || round_ops >= kRoundMaxOps) break;
         const srv_request& f = S->queued.front();
         const uint64_t oldest = fifo.empty() ? f.ticket : S->slots[fifo.front()].ticket;
         if (f.ticket - oldest >= R) break;  // no free request slot
@@ -859,21 +945,29 @@ void server_pump(mt_server* S) {
       slabs_in_use += r.demand;
       admitted_demand += r.demand;
       admitted_ops += r.n;
-      server_stage(S, r);
-      if (have_run && r.off == run_hi) {
-        run_hi += r.n;
-      } else {
-        if (have_run) rc = server_upload_range(S, run_lo, run_hi);
-        run_lo = r.off;
-        run_hi = r.off + r.n;
-        have_run = true;
-      }
+      round_ops += r.n;
       fifo.push_back(slot);
       round.slots.push_back(slot);
       progress = true;
     }
-    if (!rc && have_run) {
-      rc = server_upload_range(S, run_lo, run_hi);
+    if (!rc && !round.slots.empty()) {
+      // Copy the round's requests into the staging (in parallel when large),
+      // then upload each contiguous run of it with one copy per field.
+      auto stage = [&](size_t k) { server_stage(S, S->slots[round.slots[k]]); };
+      if (round_ops >= kPoolMinOps) S->pool.run(round.slots.size(), stage);
+      else for (size_t k = 0; k < round.slots.size(); ++k) stage(k);
+      for (uint32_t slot : round.slots) {
+        const srv_request& q = S->slots[slot];
+        if (have_run && q.off == run_hi) {
+          run_hi += q.n;
+        } else {
+          if (have_run && !rc) rc = server_upload_range(S, run_lo, run_hi);
+          run_lo = q.off;
+          run_hi = q.off + q.n;
+          have_run = true;
+        }
+      }
+      if (!rc) rc = server_upload_range(S, run_lo, run_hi);
       round.ev = take_event();
       if (!round.ev || cudaEventRecord(round.ev, S->s_up) != cudaSuccess) rc = MT_ERR_CUDA;
       if (!rc) rounds.push_back(std::move(round));
@@ -909,22 +1003,33 @@ void server_pump(mt_server* S) {
       progress = true;
     }
     // ---- completed on the device: deliver the results -------------------------
+    finished_now.clear();
+    uint64_t finished_ops = 0;
     for (size_t k = 0; !rc && k < published.size();) {
       const uint32_t slot = published[k];
       if (__atomic_load_n(&S->done[slot], __ATOMIC_ACQUIRE)) {
-        srv_request& q = S->slots[slot];
-        server_deliver(S, q);
-        q.stage = SRV_DONE;
-        completed_demand += q.demand;
-        completed_ops += q.n;
-        S->rec_latency[slot].store(now_ns(S->t0) - q.submit_ns, std::memory_order_relaxed);
-        S->rec_done[slot].store(1u, std::memory_order_release);
+        finished_now.push_back(slot);
+        finished_ops += S->slots[slot].n;
         published[k] = published.back();
         published.pop_back();
-        progress = true;
       } else {
         ++k;
       }
+    }
+    if (!finished_now.empty()) {
+      auto deliver = [&](size_t k) { server_deliver(S, S->slots[finished_now[k]]); };
+      if (finished_ops >= kPoolMinOps) S->pool.run(finished_now.size(), deliver);
+      else for (size_t k = 0; k < finished_now.size(); ++k) deliver(k);
+      const uint64_t now = now_ns(S->t0);
+      for (uint32_t slot : finished_now) {
+        srv_request& q = S->slots[slot];
+        q.stage = SRV_DONE;
+        completed_demand += q.demand;
+        completed_ops += q.n;
+        S->rec_latency[slot].store(now - q.submit_ns, std::memory_order_relaxed);
+        S->rec_done[slot].store(1u, std::memory_order_release);
+      }
+      progress = true;
     }
     while (!fifo.empty() && S->slots[fifo.front()].stage == SRV_DONE) {
       tail = std::max(tail, S->slots[fifo.front()].alloc_end);
@@ -1065,6 +1170,7 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
     return MT_ERR_CUDA;
   }
   S->t0 = clk::now();
+  S->pool.start((int)std::min(6u, std::max(1u, std::thread::hardware_concurrency() / 4u)));
   S->pump = std::thread(server_pump, S);
   *out = S;
   return MT_OK;
