@@ -376,7 +376,7 @@ def run_ours(args, rank, world, dist):
                        "max_value_length": MAXV, "tile_size": args.tile, "write_tile_size": args.write_tile,
                        "upderase_tile_size": args.upderase_tile or args.write_tile,
                        "form": "plain per-call mixed_batch (reclaim, three-way partition, find / insert / "
-                               "update+erase class kernels on forked streams)",
+                               "update+erase class kernels on forked streams, updates of one key combined)",
                        "l2": "no flush: the index (>2 GB of slabs) and each batch's inputs exceed the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "batch_latency_ms": {"p50": round(sorted_steps[len(sorted_steps) // 2], 4),
@@ -393,7 +393,9 @@ def run_ours(args, rank, world, dist):
                          "kernel": "mixed_batch call: reclaim + partition + three class kernels"},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": 5 * args.steps,  # reclaim, partition, find, insert, update/erase per step
+            # reclaim, partition, find class, insert class, update combining,
+            # update/erase class, combined results: 7 kernels per step
+            "gpu_launches": 7 * args.steps,
             "pool": {"used_slabs": stats["used_slabs"], "total_slabs": stats["total_slabs"]},
         }
         res.update(extra)

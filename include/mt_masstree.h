@@ -309,7 +309,9 @@ int mt_server_submit(mt_server* server, const uint8_t* request_types, const uint
                      const uint32_t* key_lengths, uint32_t* values, uint32_t* value_lengths, bool* results,
                      uint32_t num_ops, uint64_t* ticket);
 /* *done = 1 once the request's results are in its host buffers (then
- * *latency_ns, if not NULL, receives the time from submit to done), else 0. */
+ * *latency_ns, if not NULL, receives the time from submit to done, kept for
+ * the last 65,536 tickets or max_requests_in_flight, whichever is more; 0
+ * for older ones), else 0. */
 int mt_server_poll(mt_server* server, uint64_t ticket, int* done, uint64_t* latency_ns);
 /* Serve every submitted request, stop the loop and free the server (the tree
  * stays).  Returns the first device error of the run (as mt_sync), or

@@ -88,6 +88,66 @@ __global__ void partition3_kernel(const uint8_t* types, const uint32_t* key_leng
   }
 }
 
+// Update combining.  Updates of one key in one call have no order among each
+// other, so all but one of them can be linearised right before the one that
+// runs, and report its result: the final value is one of theirs either way.
+// Under skewed key choice this turns thousands of serialised updates of a hot
+// key (each taking the node lock) into one.  combine_kernel files every valid
+// update of the class (or of the whole call) in an open-addressing table keyed
+// by a hash of the key; the first request of a key owns its slot, the others
+// compare keys and record that request in leader_of.  The batch kernel skips
+// them, and combine_results_kernel copies the leader's result.
+MT_DEV uint64_t key_hash(const uint32_t* k, uint32_t klen) {
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ klen;
+  for (uint32_t q = 0; q < klen; ++q) {
+    h = (h ^ k[q]) * 0xFF51AFD7ED558CCDull;
+    h ^= h >> 32;
+  }
+  h *= 0xC4CEB9FE1A85EC53ull;
+  return h ^ (h >> 29);
+}
+
+MT_DEV uint32_t class_request(const batch_args& a, uint32_t pos, uint32_t nf, uint32_t nb) {
+  return a.index ? a.index[pos < nf ? pos : a.region - nb + (pos - nf)] : pos;
+}
+
+__global__ void combine_kernel(batch_args a, uint32_t* table, uint32_t mask, uint32_t* leader_of) {
+  const uint32_t nf = a.n_dev ? *a.n_dev : a.n;
+  const uint32_t nb = a.n_back_dev ? *a.n_back_dev : 0u;
+  for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < nf + nb; pos += gridDim.x * blockDim.x) {
+    const uint32_t i = class_request(a, pos, nf, nb);
+    if (a.types && a.types[i] != MT_REQ_UPDATE) continue;
+    const uint32_t klen = a.key_lengths ? a.key_lengths[i] : a.max_key_length;
+    const uint32_t vlen = a.value_lengths_in ? a.value_lengths_in[i] : a.max_value_length;
+    if (klen == 0u || klen > a.max_key_length || vlen > a.max_value_length) continue;  // reported when served
+    const uint32_t* k = a.keys + (size_t)i * a.max_key_length;
+    uint32_t slot = (uint32_t)key_hash(k, klen) & mask;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+      const uint32_t j = atomicCAS(table + slot, kInvalid, i);
+      if (j == kInvalid) break;  // i leads its key
+      const uint32_t jl = a.key_lengths ? a.key_lengths[j] : a.max_key_length;
+      bool same = jl == klen;
+      const uint32_t* kj = a.keys + (size_t)j * a.max_key_length;
+      for (uint32_t q = 0; same && q < klen; ++q) same = kj[q] == k[q];
+      if (same) {
+        leader_of[i] = j;
+        break;
+      }
+      slot = (slot + 1u) & mask;
+    }
+  }
+}
+
+__global__ void combine_results_kernel(batch_args a, const uint32_t* leader_of) {
+  const uint32_t nf = a.n_dev ? *a.n_dev : a.n;
+  const uint32_t nb = a.n_back_dev ? *a.n_back_dev : 0u;
+  for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < nf + nb; pos += gridDim.x * blockDim.x) {
+    const uint32_t i = class_request(a, pos, nf, nb);
+    const uint32_t j = leader_of[i];
+    if (j != kInvalid) a.results[i] = a.results[j];
+  }
+}
+
 template <int T, int OP, bool CONC>
 __global__ void __launch_bounds__(kBlock, min_blocks_for<OP>) batch_kernel(tree_view tv, batch_args a) {
   tile<T> t;
@@ -323,6 +383,14 @@ int launch_batch(mt_masstree* t, const batch_args& a, cudaStream_t s) {
   return launch_batch_tile<OP, CONC>(t, OP == OP_FIND ? t->tile_size : t->write_tile_size, a, s);
 }
 
+// Slots of the update-combining table for n requests: a power of two of at
+// least 2n (load factor at most one half).
+uint32_t combine_slots(uint32_t n) {
+  uint32_t p = 64;
+  while (p < 2u * n && p < (1u << 31)) p <<= 1;
+  return p;
+}
+
 // Index scratch for split mixed batches (grown on demand, kept).
 int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   if (n <= t->split_cap) return MT_OK;
@@ -331,9 +399,34 @@ int ensure_split_scratch(mt_masstree* t, uint32_t n, cudaStream_t s) {
   t->split_idx = nullptr;
   t->split_cap = 0;
   // [counts(32 words, one line)] [find indices n] [insert indices n] [update/erase indices n]
-  if (cudaMalloc(&t->split_idx, (32u + 3ull * n) * sizeof(uint32_t)) != cudaSuccess) return MT_ERR_OOM;
+  // [leader_of n] [combining table combine_slots(n)]
+  if (cudaMalloc(&t->split_idx, (32u + 4ull * n + combine_slots(n)) * sizeof(uint32_t)) != cudaSuccess)
+    return MT_ERR_OOM;
   t->split_cap = n;
   return MT_OK;
+}
+
+// Combine the updates among the requests `a` describes (a class of a mixed
+// batch, or a whole update call) on stream s; returns a.leader_of for the batch
+// kernel (nullptr when there is nothing to combine into).
+int launch_combine(mt_masstree* t, batch_args& a, uint32_t n, cudaStream_t s) {
+  uint32_t* leader_of = t->split_idx + 32 + 3ull * t->split_cap;
+  uint32_t* table = leader_of + t->split_cap;
+  const uint32_t slots = combine_slots(n);
+  if (cudaMemsetAsync(leader_of, 0xFF, (size_t)n * sizeof(uint32_t), s) != cudaSuccess ||
+      cudaMemsetAsync(table, 0xFF, (size_t)slots * sizeof(uint32_t), s) != cudaSuccess)
+    return MT_ERR_CUDA;
+  combine_kernel<<<std::max(1, std::min(t->sms * 8, (int)((n + 255) / 256))), 256, 0, s>>>(a, table, slots - 1u,
+                                                                                           leader_of);
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
+  a.leader_of = leader_of;
+  return MT_OK;
+}
+
+int launch_combine_results(mt_masstree* t, const batch_args& a, uint32_t n, cudaStream_t s) {
+  if (!a.results || !a.leader_of) return MT_OK;
+  combine_results_kernel<<<std::max(1, std::min(t->sms * 8, (int)((n + 255) / 256))), 256, 0, s>>>(a, a.leader_of);
+  return cuda_status(cudaGetLastError());
 }
 
 int launch_mixed_split(mt_masstree* t, batch_args a, bool bucket_keys, cudaStream_t s) {
@@ -373,7 +466,9 @@ int launch_mixed_split(mt_masstree* t, batch_args a, bool bucket_keys, cudaStrea
   const uint32_t tu = t->upderase_tile_size ? t->upderase_tile_size : tw;
   rc = launch_batch_tile<OP_PASS_INSERT, true>(t, tw, i, s);
   if (!rc) rc = launch_batch_tile<OP_FIND, true>(t, t->tile_size, f, t->side[0]);
+  if (!rc) rc = launch_combine(t, u, a.n, t->side[1]);
   if (!rc) rc = launch_batch_tile<OP_PASS_UPDERASE, true>(t, tu, u, t->side[1]);
+  if (!rc) rc = launch_combine_results(t, u, a.n, t->side[1]);
   return host_join(t, s, rc);
 }
 
@@ -601,7 +696,13 @@ int mt_update(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_
   batch_args a{};
   a.keys = keys; a.key_lengths = klens; a.values = const_cast<uint32_t*>(values); a.value_lengths_in = vlens;
   a.results = results; a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
-  return launch_batch<OP_UPDATE, true>(t, a, (cudaStream_t)stream);
+  const cudaStream_t s = (cudaStream_t)stream;
+  if (n < 2) return launch_batch<OP_UPDATE, true>(t, a, s);
+  int rc = ensure_split_scratch(t, n, s);
+  if (!rc) rc = launch_combine(t, a, n, s);
+  if (!rc) rc = launch_batch<OP_UPDATE, true>(t, a, s);
+  if (!rc) rc = launch_combine_results(t, a, n, s);
+  return rc;
 }
 
 int mt_erase(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_t* klens, uint32_t n,

@@ -47,6 +47,8 @@ struct batch_args {
   uint32_t* value_lengths_out;
   bool* results;
   uint32_t* values_out;          // optional: find outputs go here instead of `values` (same row stride)
+  const uint32_t* leader_of;     // optional: per request, the request it was combined into (kInvalid: none);
+                                 // combined requests are not served here (combine_results_kernel copies results)
   const uint32_t* index;       // optional request subset
   const uint32_t* n_dev;       // optional device-side request count (with index)
   const uint32_t* n_back_dev;  // optional: further indices at the END of the index region
@@ -145,10 +147,11 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
     // caller's buffers: such requests are skipped and reported.
     const bool bad = valid && (klen > a.max_key_length || vlen > a.max_value_length || kind > MT_REQ_UPDATE);
     if (t.any(bad) && bad) record_error(tv.pool, ERR_INVALID_ARG);
+    const bool combined = valid && a.leader_of != nullptr && a.leader_of[i] != kInvalid;
     uint32_t res = 0, vout = 0;
     const uint32_t nreq = min(per, n - base);
     for (uint32_t r = 0; r < nreq; ++r) {
-      if (t.shfl((uint32_t)bad, (int)r)) continue;
+      if (t.shfl((uint32_t)(bad || combined), (int)r)) continue;
       const uint32_t j = t.shfl(i, (int)r);
       const uint32_t k = t.shfl(kind, (int)r);
       const uint32_t kl = t.shfl(klen, (int)r);
@@ -157,7 +160,7 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
       run_request<T, OP, CONC>(t, tv, cache, a, j, k, kl, vl, rr, vo);
       if (t.rank == r) { res = rr; vout = vo; }
     }
-    if (valid) {
+    if (valid && !combined) {
       if (kind == MT_REQ_FIND) {
         if (a.value_lengths_out) a.value_lengths_out[i] = vout;
       } else if (a.results) {

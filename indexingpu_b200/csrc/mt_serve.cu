@@ -725,6 +725,7 @@ struct mt_server {
   mt_masstree* tree = nullptr;
   mt_server_config cfg{};
   uint32_t C = 0, R = 0;
+  uint32_t L = 0;  // completion records: ticket % L (at least 65,536 tickets back, whatever R)
   // Device staging of the inputs, and its pinned host mirror.
   void* dmem = nullptr;
   uint8_t* d_types = nullptr;
@@ -940,8 +941,9 @@ void server_pump(mt_server* S) {
       const uint32_t slot = (uint32_t)(r.ticket % R);
       r.stage = SRV_UPLOADING;
       S->slots[slot] = r;
-      S->rec_done[slot].store(0u, std::memory_order_relaxed);
-      S->rec_ticket[slot].store(r.ticket, std::memory_order_release);
+      const uint32_t rec = (uint32_t)(r.ticket % S->L);
+      S->rec_done[rec].store(0u, std::memory_order_relaxed);
+      S->rec_ticket[rec].store(r.ticket, std::memory_order_release);
       slabs_in_use += r.demand;
       admitted_demand += r.demand;
       admitted_ops += r.n;
@@ -1026,8 +1028,9 @@ void server_pump(mt_server* S) {
         q.stage = SRV_DONE;
         completed_demand += q.demand;
         completed_ops += q.n;
-        S->rec_latency[slot].store(now - q.submit_ns, std::memory_order_relaxed);
-        S->rec_done[slot].store(1u, std::memory_order_release);
+        const uint32_t rec = (uint32_t)(q.ticket % S->L);
+        S->rec_latency[rec].store(now - q.submit_ns, std::memory_order_relaxed);
+        S->rec_done[rec].store(1u, std::memory_order_release);
       }
       progress = true;
     }
@@ -1080,6 +1083,7 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
   S->cfg = *cfg;
   S->C = cfg->max_ops_in_flight ? cfg->max_ops_in_flight : (1u << 20);
   S->R = cfg->max_requests_in_flight ? cfg->max_requests_in_flight : 65536u;
+  S->L = std::max<uint32_t>(S->R, 65536u);
   const uint32_t C = S->C, R = S->R, K = cfg->max_key_length, V = cfg->max_value_length;
   auto up = [](size_t b) { return (b + 255u) & ~size_t(255); };
   const size_t bytes = up(C) + up((size_t)C * K * 4u) + 3 * up((size_t)C * 4u) + up((size_t)C * V * 4u);
@@ -1123,11 +1127,11 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
        cudaStreamCreateWithFlags(&S->s_up, cudaStreamNonBlocking) == cudaSuccess;
   if (ok) {
     S->slots.resize(R);
-    S->rec_ticket.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
-    S->rec_done.reset(new (std::nothrow) std::atomic<uint32_t>[R]);
-    S->rec_latency.reset(new (std::nothrow) std::atomic<uint64_t>[R]);
+    S->rec_ticket.reset(new (std::nothrow) std::atomic<uint64_t>[S->L]);
+    S->rec_done.reset(new (std::nothrow) std::atomic<uint32_t>[S->L]);
+    S->rec_latency.reset(new (std::nothrow) std::atomic<uint64_t>[S->L]);
     ok = S->rec_ticket && S->rec_done && S->rec_latency;
-    for (uint32_t k = 0; ok && k < R; ++k) {
+    for (uint32_t k = 0; ok && k < S->L; ++k) {
       S->rec_ticket[k].store(0);
       S->rec_done[k].store(0);
       S->rec_latency[k].store(0);
@@ -1201,15 +1205,15 @@ extern "C" int mt_server_submit(mt_server* S, const uint8_t* types, const uint32
 
 extern "C" int mt_server_poll(mt_server* S, uint64_t ticket, int* done, uint64_t* latency_ns) {
   if (!S || !done || ticket >= S->next_ticket.load(std::memory_order_acquire)) return MT_ERR_INVALID_ARG;
-  const uint32_t slot = (uint32_t)(ticket % S->R);
-  const uint64_t rt = S->rec_ticket[slot].load(std::memory_order_acquire);
+  const uint32_t rec = (uint32_t)(ticket % S->L);
+  const uint64_t rt = S->rec_ticket[rec].load(std::memory_order_acquire);
   *done = 0;
   if (latency_ns) *latency_ns = 0;
   if (rt > ticket) {
-    *done = 1;  // the slot moved on to a later request: this one completed (its latency is gone)
-  } else if (rt == ticket && S->rec_done[slot].load(std::memory_order_acquire)) {
+    *done = 1;  // the record moved on to a later request: this one completed (its latency is gone)
+  } else if (rt == ticket && S->rec_done[rec].load(std::memory_order_acquire)) {
     *done = 1;
-    if (latency_ns) *latency_ns = S->rec_latency[slot].load(std::memory_order_relaxed);
+    if (latency_ns) *latency_ns = S->rec_latency[rec].load(std::memory_order_relaxed);
   }
   if (!*done) {
     const int st = S->status.load(std::memory_order_acquire);

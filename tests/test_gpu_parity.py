@@ -5,7 +5,7 @@ Integer results must match bit-for-bit.
 import numpy as np
 import pytest
 
-from indexes import GpuIndex, OracleIndex
+from indexes import GpuIndex, OracleIndex, same_state
 from indexingpu_b200 import workload as wl
 from scenarios import assert_found
 
@@ -262,5 +262,56 @@ def test_scan_layers_beyond_scratch(tile, depth):
         g.t.reclaim()
         st = g.t.stats()
         assert st["limbo_slabs"] == 0 and st["device_error"] == 0
+    finally:
+        g.close()
+
+
+def test_combined_updates_of_hot_keys(tile):
+    # Many updates of few keys in one call (what skewed key choice gives): all
+    # but one per key are combined into the one that runs and report its
+    # result.  Keys present and not erased in the call: every update true;
+    # absent keys: every update false; the final contents are the oracle's
+    # (the update values of one key are equal, as in the benchmark streams).
+    c2 = wl.C2(n_preload=5000, n_prefixes=64)
+    k, l, v, vl = c2.keys(np.arange(5000))
+    g, o = GpuIndex(tile), OracleIndex()
+    try:
+        g.insert(k, l, v, vl)
+        o.insert(k, l, v, vl)
+        rng = np.random.default_rng(tile)
+        hot = rng.choice(3000, 40, replace=False)  # none of the keys erased below
+        absent_k, absent_l, _, _ = c2.keys(np.arange(6000, 6010))
+        ids = np.concatenate([np.repeat(hot, 300), np.arange(3000, 3200)])
+        uk = np.concatenate([k[ids], np.repeat(absent_k, 50, axis=0)])
+        ul = np.concatenate([l[ids], np.repeat(absent_l, 50)])
+        uv = np.concatenate([v[ids] ^ np.uint32(0x77), np.zeros((500, 8), np.uint32)])
+        uvl = np.concatenate([vl[ids], np.full(500, 3, np.uint32)])
+        perm = rng.permutation(len(uk))
+        uk, ul, uv, uvl = uk[perm], ul[perm], uv[perm], uvl[perm]
+        rg = g.update(uk, ul, uv, uvl)
+        ro = o.update(uk, ul, uv, uvl)
+        np.testing.assert_array_equal(rg, ro)  # present: true, absent: false, whatever the order
+        same_state(g, o, 16, 8)
+        # The same inside mixed batches, with finds of the hot keys, and erases
+        # of other keys' duplicates (their updates may go either way).
+        types = np.full(len(uk), wl.REQ_UPDATE, np.uint8)
+        fk = k[hot]
+        erase_ids = np.arange(3200, 3260)
+        bk = np.concatenate([uk, fk, k[erase_ids], k[erase_ids]])
+        bl = np.concatenate([ul, l[hot], l[erase_ids], l[erase_ids]])
+        bv = np.concatenate([uv ^ np.uint32(1), np.zeros((len(hot) + 120, 8), np.uint32)])
+        bvl = np.concatenate([uvl, np.zeros(len(hot) + 120, np.uint32)])
+        bt = np.concatenate([types, np.full(len(hot), wl.REQ_FIND, np.uint8), np.full(60, wl.REQ_ERASE, np.uint8),
+                             np.full(60, wl.REQ_UPDATE, np.uint8)])
+        bv[-60:] = 5
+        bvl[-60:] = 2
+        gv, gl, gr = g.mixed(bt, bk, bl, bv, bvl)
+        o.mixed(bt, bk, bl, bv, bvl)
+        n_upd = len(uk)
+        np.testing.assert_array_equal(gr[:n_upd], rg)  # the hot keys stay present: same results as before
+        assert (gl[n_upd:n_upd + len(hot)] > 0).all()
+        same_state(g, o, 16, 8)
+        ok, nkeys, msg = g.t.validate()
+        assert ok and nkeys == o.o.size(), msg
     finally:
         g.close()

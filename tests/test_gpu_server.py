@@ -114,7 +114,10 @@ def test_online_server_alone_and_in_the_mix(tile, chunk):
             # the ring wraps and admission waits for earlier requests.
             cfg = dict(chunk_ops=chunk) if alone else dict(chunk_ops=chunk, max_ops_in_flight=2048,
                                                            max_requests_in_flight=32)
+            t0 = time.time()
             got = _serve_online(torch, g, st, alone, **cfg)
+            print(f"tile {tile} chunk {chunk} alone={alone}: {time.time() - t0:.3f} s, "
+                  f"latency p50 {np.percentile(got[3], 50) / 1e3:.1f} us, max {got[3].max() / 1e3:.1f} us")
             _check(st, got, exp)
             assert (got[3] > 0).all()
             o.mixed(st["types"], st["keys"], st["lens"], st["vals"], st["vlens"])
