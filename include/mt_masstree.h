@@ -54,17 +54,21 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
                                        every request class */
 #define MT_FLAG_PERSISTENT 32u      /* mixed_batches: one cooperative persistent launch for all
                                        sub-batches instead of three class kernels per sub-batch */
-#define MT_FLAG_MERGE 64u           /* erase, mixed_batch: after the call's erases, fold border
-                                       nodes left with 4 entries or fewer into a neighbour under
-                                       the same parent (reference erase merge levels 2-4; space
-                                       only, results are the same) */
+#define MT_FLAG_MERGE 64u           /* erase, mixed_batch: after the call's erases, fold nodes
+                                       left with 4 entries or fewer into a neighbour under the same
+                                       parent, border nodes and then their sparse ancestors, and
+                                       fold a layer root left with one child into its slab
+                                       (reference erase merge levels 2-4; space only, results are
+                                       the same) */
 #define MT_FLAG_INPUTS_ON_STREAM 256u /* mixed_batch_host: the uploads wait for the work queued on `stream`
                                        before the call (for host inputs that work produces, e.g. a copy
                                        queued just before); without it the uploads start at once */
 #define MT_FLAG_REMOVE_EMPTY_LAYERS 128u /* erase, mixed_batch: after the call's erases (and merges),
                                        remove every trie layer (1 or deeper, reached by at most 15
-                                       key slices) whose only node they left empty, and the parent
-                                       layers this empties in turn (reference erase merge level 4,
+                                       key slices) whose only node they left empty (with
+                                       MT_FLAG_MERGE: whose nodes all folded into an empty root),
+                                       and the parent layers this empties in turn (reference erase
+                                       merge level 4,
                                        do_remove_empty_root, include/gpu_masstree.hpp:914-960;
                                        space only, results are the same) */
 

@@ -33,18 +33,28 @@ def build(force=False, verbose=True, extra_flags=()):
     deps.append(os.path.join(ROOT, "include", "mt_masstree.h"))
     if not force and not _stale(LIB, deps):
         return LIB
-    # One object per translation unit, compiled in parallel, then linked.
+    # One object per translation unit, compiled in parallel, then linked; an
+    # object newer than its source and every header, and built with the same
+    # flags, is kept.
+    headers = [d for d in deps if not d.endswith(".cu")]
+    stamp = os.path.join(CSRC, ".objects_built_with")
+    flags = " ".join([*NVCC_FLAGS, *extra_flags])
+    same_flags = os.path.exists(stamp) and open(stamp).read() == flags
     objs, procs = [], []
     for src in SOURCES:
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        objs.append(obj)
+        if not force and same_flags and not _stale(obj, [os.path.join(CSRC, src), *headers]):
+            continue
         cmd = ["nvcc", *NVCC_FLAGS, *extra_flags, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append(subprocess.Popen(cmd))
-        objs.append(obj)
     for pr in procs:
         if pr.wait() != 0:
             raise subprocess.CalledProcessError(pr.returncode, "nvcc")
+    with open(stamp, "w") as f:
+        f.write(flags)
     link = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(link), flush=True)

@@ -885,13 +885,23 @@ struct validator {
   }
 
   // Validate the subtree at idx covering (lo, hi] (lo exclusive unless first).
-  bool subtree(uint32_t idx, uint64_t lo_excl, uint32_t hi, int level, int& border_level, int layer_depth) {
+  // last[level] is the node met before at that level of the layer (in key
+  // order), whose sibling link must lead to this one.
+  bool subtree(uint32_t idx, uint64_t lo_excl, uint32_t hi, int level, int& border_level, int layer_depth,
+               std::vector<uint32_t>& last) {
     if (!ok(idx)) return fail("node index out of range");
     if (!mark(idx)) return false;
     const uint32_t* w = slab(idx);
     const uint32_t meta = w[WORD_META], ks = w[WORD_KS], n = meta & META_COUNT;
     ++nodes;
     if (meta & META_LOCK) return fail("node left locked");
+    if (meta & META_DEAD) return fail("merged-away node still linked");
+    if ((size_t)level >= last.size()) last.resize((size_t)level + 1u, kInvalid);
+    if (last[level] != kInvalid) {
+      const uint32_t* pw = slab(last[level]);
+      if (!(pw[WORD_META] & META_SIB) || pw[WORD_SIB] != idx) return fail("sibling link does not lead to the next node");
+    }
+    last[level] = idx;
     if (n > (uint32_t)kMaxEntries) return fail("count above the node capacity");
     if (node_checksum(w) != w[WORD_CSUM]) return fail("node checksum mismatch");
     if (w[WORD_HIGH] != hi) return fail("high key differs from the parent's separator");
@@ -925,7 +935,7 @@ struct validator {
     for (uint32_t e = 0; e < n; ++e) {
       const uint32_t sep = w[2 * e];
       if (lo != ~0ull && (uint64_t)sep <= lo) return fail("interior separators out of order");
-      if (!subtree(w[2 * e + 1], lo, sep, level + 1, border_level, layer_depth)) return false;
+      if (!subtree(w[2 * e + 1], lo, sep, level + 1, border_level, layer_depth, last)) return false;
       lo = sep;
     }
     if (w[2 * (n - 1)] != hi) return fail("last separator differs from the high key");
@@ -937,7 +947,11 @@ struct validator {
     if (!ok(root)) return fail("layer root out of range");
     if (!(slab(root)[WORD_META] & META_ROOT)) return fail("layer root without ROOT flag");
     int border_level = -1;
-    return subtree(root, ~0ull, 0xFFFFFFFFu, 0, border_level, depth);
+    std::vector<uint32_t> last;
+    if (!subtree(root, ~0ull, 0xFFFFFFFFu, 0, border_level, depth, last)) return false;
+    for (uint32_t i : last)
+      if (slab(i)[WORD_META] & META_SIB) return fail("rightmost node of a level with a sibling link");
+    return true;
   }
 };
 

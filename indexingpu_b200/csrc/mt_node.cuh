@@ -10,7 +10,7 @@
 //   word 28       : high key (largest slice this node covers; 0xFFFFFFFF for the
 //                   rightmost node of a level)
 //   word 29       : right sibling slab (valid iff META_SIB)
-//   word 30       : meta  = count:4 | LOCK | BORDER | SIB | ROOT | version:16 (bits 16..31)
+//   word 30       : meta  = count:4 | LOCK | BORDER | SIB | ROOT | DEAD | version:16 (bits 16..31)
 //   word 31       : keystates of a border node, 2 bits per entry
 //
 // Why a checksum: on B200 a 128-byte line stored by one warp instruction is
@@ -49,6 +49,10 @@ constexpr uint32_t META_LOCK = 1u << 4;
 constexpr uint32_t META_BORDER = 1u << 5;
 constexpr uint32_t META_SIB = 1u << 6;
 constexpr uint32_t META_ROOT = 1u << 7;
+// Set on the last image of a node that a merge folded into another one: a pass
+// that locks a node through a stale path sees that it no longer belongs to the
+// tree.  (Nothing else reads it; the slab is reused only after the launch.)
+constexpr uint32_t META_DEAD = 1u << 8;
 constexpr uint32_t META_VERSION_ONE = 1u << 16;
 
 constexpr int WORD_CSUM = 26, WORD_HIGH = 28, WORD_SIB = 29, WORD_META = 30, WORD_KS = 31;
@@ -122,6 +126,7 @@ struct node {
   MT_DEV bool is_root() const { return (meta & META_ROOT) != 0u; }
   MT_DEV bool has_sib() const { return (meta & META_SIB) != 0u; }
   MT_DEV bool locked() const { return (meta & META_LOCK) != 0u; }
+  MT_DEV bool dead() const { return (meta & META_DEAD) != 0u; }
   MT_DEV bool full() const { return count() >= (uint32_t)kMaxEntries; }
   // B-link move-right test: the slice lies beyond this node.
   MT_DEV bool must_move_right(uint32_t slice) const { return has_sib() && slice > high; }

@@ -65,7 +65,8 @@ struct tree_view {
   // Layer log of the current call, null unless the call removes the trie
   // layers that its erases empty: [0] records, [1] unused, then records of
   // kLayerRecWords words, {layer, key slices 0 .. layer-1}, one per erase
-  // that left the only node of a layer (layer 1 or deeper) without entries.
+  // that left the only node of a layer (layer 1 or deeper) without entries,
+  // or (when the call merges too) the layer's rightmost border node.
   uint32_t* layer_log;
   uint32_t layer_cap;
 };
@@ -75,7 +76,8 @@ struct tree_view {
 constexpr uint32_t kLayerRecWords = 16;
 
 // A border node with this many entries or fewer after an erase is a merge
-// candidate (of kMaxEntries = 13).
+// candidate (of kMaxEntries = 13), and so is an interior node that a merge
+// of its children leaves with this many.
 constexpr uint32_t kMergeAt = 4;
 
 // ---- locking -----------------------------------------------------------------
@@ -733,8 +735,10 @@ MT_DEV int coop_erase(const tile<T>& t, const tree_view& tv, const uint32_t* key
         tv.merge_log[3u + 2u * r] = slice;
       }
     }
-    if (tv.layer_log != nullptr && t.leader() && layer >= 1u && layer < kLayerRecWords && nd.is_root() &&
-        nd.count() == 0u && !nd.has_sib()) {
+    // A layer's empty root is logged for removal; with merges also its emptied
+    // rightmost border node, as the merges may fold the layer into its root.
+    if (tv.layer_log != nullptr && t.leader() && layer >= 1u && layer < kLayerRecWords && nd.count() == 0u &&
+        !nd.has_sib() && (nd.is_root() || tv.merge_log != nullptr)) {
       const uint32_t r = atomicAdd(tv.layer_log, 1u);
       if (r < tv.layer_cap) {
         uint32_t* rec = tv.layer_log + 2u + (size_t)kLayerRecWords * r;

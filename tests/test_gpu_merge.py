@@ -1,8 +1,10 @@
 """Erase with MT_FLAG_MERGE (the reference's erase merge levels 2-4): sparse
-border nodes are folded into a neighbour after the call's erases.  Results and
-the full ordered contents must equal the oracle's and the tree must validate,
-through later inserts, finds and mixed batches too; the merged tree must hold
-fewer slabs than the same tree erased without merges."""
+border nodes, and then sparse interior nodes, are folded into a neighbour after
+the call's erases, and a layer root left with one child takes it in.  Results
+and the full ordered contents must equal the oracle's and the tree must
+validate (sibling links included), through later inserts, finds and mixed
+batches too; the merged tree must hold fewer slabs than the same tree erased
+without merges."""
 import numpy as np
 import pytest
 
@@ -200,8 +202,82 @@ def test_remove_emptied_layers():
         ok, nkeys, report = gr.t.validate()
         assert ok, report
         assert nkeys == 0
-        assert _used(gr) < 400, (_used(gr), full)
+        # Layer 0 lost its LINK entries in the removal pass; merged upwards,
+        # it folded back into its root.
+        assert _used(gr) == 1, (_used(gr), full)
         same_state(gr, o, 4, 8)
     finally:
         gr.close()
         g0.close()
+
+
+def _one_layer_keys(n, seed):
+    """n distinct one-slice keys with one-slice values (every entry inline in
+    layer 0)."""
+    rng = np.random.default_rng(seed)
+    s = np.unique(rng.integers(0, 1 << 32, 2 * n, dtype=np.uint64).astype(np.uint32))[:n]
+    rng.shuffle(s)
+    keys = s.reshape(n, 1).copy()
+    vals = rng.integers(0, 1 << 32, (n, 1), dtype=np.uint64).astype(np.uint32)
+    return keys, np.ones(n, np.uint32), vals, np.ones(n, np.uint32)
+
+
+@pytest.mark.parametrize("write_tile", [8, 32])
+def test_interior_merges_and_root_collapse(write_tile):
+    """300,000 one-slice keys grown by splits (a layer of six levels), 96%
+    erased in three calls: interior nodes merge as well as border nodes, so
+    the merged tree holds few more slabs than a tree built from the surviving
+    keys alone.  Erasing the rest folds the layer back into its root slab (one
+    slab in use); the keys then go back in."""
+    n = 300000
+    keys, lens, vals, vlens = _one_layer_keys(n, 31)
+    gm, g0, gf, o = (GpuIndex(tile_size=8, pool_bytes=256 << 20), GpuIndex(tile_size=8, pool_bytes=256 << 20),
+                     GpuIndex(tile_size=8, pool_bytes=256 << 20), OracleIndex())
+    try:
+        for g in (gm, g0):
+            g.t.set_write_tile_size(write_tile)
+            for a in range(0, n, 30000):
+                g.insert(keys[a:a + 30000], lens[a:a + 30000], vals[a:a + 30000], vlens[a:a + 30000])
+        o.insert(keys, lens, vals, vlens)
+        rng = np.random.default_rng(32)
+        perm = rng.permutation(n)
+        gone, kept = perm[: n * 96 // 100], perm[n * 96 // 100:]
+        for part in np.array_split(gone, 3):
+            ro = o.erase(keys[part], lens[part])
+            np.testing.assert_array_equal(gm.erase(keys[part], lens[part], merge=True), ro)
+            np.testing.assert_array_equal(g0.erase(keys[part], lens[part]), ro)
+            ok, nkeys, report = gm.t.validate()
+            assert ok, report
+        gf.insert(keys[kept], lens[kept], vals[kept], vlens[kept])
+        assert nkeys == len(kept)
+        same_state(gm, o, 1, 1)
+        used_m, used_0, used_f = _used(gm), _used(g0), _used(gf)
+        print(f"slabs after 96% erased: merged {used_m}, unmerged {used_0}, built from the rest {used_f}")
+        assert used_m < 2 * used_f, (used_m, used_f)
+        gv, gl = gm.find(keys, lens, 1)
+        ov, ol = o.find(keys, lens, 1)
+        assert_found(gv, gl, ov, ol, "finds on the merged tree")
+        # Everything else erased (with a mixed batch of finds beside): one slab.
+        types = np.concatenate([np.full(len(kept), wl.REQ_ERASE, np.uint8), np.full(1000, wl.REQ_FIND, np.uint8)])
+        idx = np.concatenate([kept, gone[:1000]])
+        sh = rng.permutation(len(idx))
+        types, idx = types[sh], idx[sh]
+        vl = np.where(types == wl.REQ_FIND, 0, 1).astype(np.uint32)
+        gv, gl, gr = gm.mixed(types, keys[idx], lens[idx], vals[idx], vl, merge=True)
+        ov, ol, orr = o.mixed(types, keys[idx], lens[idx], vals[idx], vl)
+        nf = types != wl.REQ_FIND
+        np.testing.assert_array_equal(gr[nf], orr[nf])
+        assert_found(gv[~nf], gl[~nf], ov[~nf], ol[~nf], "finds beside the last erases")
+        ok, nkeys, report = gm.t.validate()
+        assert ok, report
+        assert nkeys == 0
+        assert _used(gm) == 1, _used(gm)
+        np.testing.assert_array_equal(gm.insert(keys, lens, vals, vlens), o.insert(keys, lens, vals, vlens))
+        ok, nkeys, report = gm.t.validate()
+        assert ok, report
+        assert nkeys == n
+        same_state(gm, o, 1, 1)
+    finally:
+        gm.close()
+        g0.close()
+        gf.close()
