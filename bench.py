@@ -535,10 +535,16 @@ def run_served(args, tree, c2, stream):
         tree.sync(stream)
         ops = int(st["nops"].sum())
         p = np.percentile(lat / 1e3, [50, 99, 99.9])
-        return {"offered_req_s": None if rate is None else round(rate, 1), "requests": n_req, "ops": ops,
-                "req_s": round(n_req / (stats["wall_ns"] / 1e9), 1), "mops": round(ops / stats["wall_ns"] * 1e3, 3),
-                "p50_us": round(float(p[0]), 1), "p99_us": round(float(p[1]), 1), "p999_us": round(float(p[2]), 1),
-                "admission_waits": stats["admission_waits"]}
+        r = {"offered_req_s": None if rate is None else round(rate, 1), "requests": n_req, "ops": ops,
+             "req_s": round(n_req / (stats["wall_ns"] / 1e9), 1), "mops": round(ops / stats["wall_ns"] * 1e3, 3),
+             "p50_us": round(float(p[0]), 1), "p99_us": round(float(p[1]), 1), "p999_us": round(float(p[2]), 1),
+             "admission_waits": stats["admission_waits"]}
+        if online:
+            # Mean time per stage of the server (submit -> admitted -> uploaded
+            # and published -> completion flag seen -> results delivered).
+            r["stage_mean_us"] = {k: round(v / 1e3 / max(1, stats["requests_done"]), 1)
+                                  for k, v in stats["stage_ns"].items()}
+        return r
 
     peak = once(0, None)
     curve = []

@@ -264,6 +264,8 @@ typedef struct mt_serve_stats {
   uint64_t requests_done;
   uint64_t ops_done;
   uint64_t admission_waits;  /* times an arrived request waited for slab memory */
+  uint64_t stage_ns[4];      /* MT_SERVE_ONLINE: the server's queued / upload / device /
+                                deliver sums (mt_server_stats_t); 0 otherwise */
 } mt_serve_stats;
 
 /* Serve an open-loop stream of requests: each request is admitted when its
@@ -317,6 +319,24 @@ int mt_server_submit(mt_server* server, const uint8_t* request_types, const uint
  * the last 65,536 tickets or max_requests_in_flight, whichever is more; 0
  * for older ones), else 0. */
 int mt_server_poll(mt_server* server, uint64_t ticket, int* done, uint64_t* latency_ns);
+/* Where completed requests spent their time: sums over the requests completed
+ * so far (divide by `requests` for means) of the time from submit to
+ * admission (queued behind earlier requests, staging space or the memory
+ * budget), admission to publication (the copy into the staging and its upload),
+ * publication to the device's completion flag as the host thread saw it, and
+ * flag to results in the caller's buffers; and the largest submit-to-done
+ * time. */
+typedef struct mt_server_stats_t {
+  uint64_t requests;
+  uint64_t ops;
+  uint64_t queued_ns;
+  uint64_t upload_ns;
+  uint64_t device_ns;
+  uint64_t deliver_ns;
+  uint64_t max_latency_ns;
+  uint64_t reserved;
+} mt_server_stats_t;
+int mt_server_stats(mt_server* server, mt_server_stats_t* out);
 /* Serve every submitted request, stop the loop and free the server (the tree
  * stays).  Returns the first device error of the run (as mt_sync), or
  * MT_ERR_LOCK_TIMEOUT if the queued work did not drain within 60 s. */

@@ -44,6 +44,7 @@ SIGNATURES = {
     "mt_server_submit": (_int, [_p, _p, _p, _p, _p, _p, _p, _u32, ctypes.POINTER(_u64)]),
     "mt_server_poll": (_int, [_p, _u64, ctypes.POINTER(_int), ctypes.POINTER(_u64)]),
     "mt_server_stop": (_int, [_p]),
+    "mt_server_stats": (_int, [_p, _p]),
 }
 
 
@@ -103,6 +104,20 @@ class MtServeStats(ctypes.Structure):
         ("requests_done", _u64),
         ("ops_done", _u64),
         ("admission_waits", _u64),
+        ("stage_ns", _u64 * 4),
+    ]
+
+
+class MtServerStats(ctypes.Structure):
+    _fields_ = [
+        ("requests", _u64),
+        ("ops", _u64),
+        ("queued_ns", _u64),
+        ("upload_ns", _u64),
+        ("device_ns", _u64),
+        ("deliver_ns", _u64),
+        ("max_latency_ns", _u64),
+        ("reserved", _u64),
     ]
 
 

@@ -593,6 +593,7 @@ extern "C" int mt_serve(mt_masstree* t, const mt_serve_plan* plan, uint64_t* lat
     stats->requests_done = admitted;
     stats->ops_done = ops_done;
     stats->admission_waits = rejected_waits;
+    for (uint64_t& x : stats->stage_ns) x = 0;
   }
   if (!rc) rc = mt_sync(t, nullptr);
   return rc;
@@ -626,6 +627,7 @@ struct srv_request {
   bool* results = nullptr;
   uint32_t n = 0;
   uint64_t submit_ns = 0;
+  uint64_t admit_ns = 0, publish_ns = 0, done_ns = 0;  // stage times (mt_server_stats)
   uint32_t off = 0;        // staging offset of the request's ops
   uint64_t alloc_end = 0;  // staging head after its allocation
   uint32_t demand = 0;     // slab demand estimate
@@ -762,6 +764,9 @@ struct mt_server {
   std::atomic<bool> exited{false};    // the pump has ended
   std::atomic<int> status{MT_OK};
   clk::time_point t0;
+  // Stage sums of completed requests (written by the pump, read by mt_server_stats).
+  std::atomic<uint64_t> st_requests{0}, st_ops{0}, st_queued{0}, st_upload{0}, st_device{0}, st_deliver{0},
+      st_max{0};
 };
 
 namespace {
@@ -907,6 +912,7 @@ void server_pump(mt_server* S) {
     uint64_t round_ops = 0;
     uint32_t run_lo = 0, run_hi = 0;  // current contiguous staging run
     bool have_run = false;
+    const uint64_t round_ns = now_ns(S->t0);
     while (!rc) {
       srv_request r;
       {
@@ -940,6 +946,7 @@ void server_pump(mt_server* S) {
       }
       const uint32_t slot = (uint32_t)(r.ticket % R);
       r.stage = SRV_UPLOADING;
+      r.admit_ns = round_ns;
       S->slots[slot] = r;
       const uint32_t rec = (uint32_t)(r.ticket % S->L);
       S->rec_done[rec].store(0u, std::memory_order_relaxed);
@@ -977,6 +984,7 @@ void server_pump(mt_server* S) {
     // ---- publish uploaded rounds as work items --------------------------------
     while (!rc && !rounds.empty() && cudaEventQuery(rounds.front().ev) == cudaSuccess) {
       srv_round& rd = rounds.front();
+      const uint64_t pub_ns = now_ns(S->t0);
       for (uint32_t slot : rd.slots) {
         srv_request& q = S->slots[slot];
         uint32_t chunk = fixed_chunk;
@@ -997,6 +1005,7 @@ void server_pump(mt_server* S) {
           left -= c;
         }
         q.stage = SRV_PUBLISHED;
+        q.publish_ns = pub_ns;
         published.push_back(slot);
       }
       __atomic_store_n(S->pub, (unsigned long long)items_published, __ATOMIC_RELEASE);
@@ -1007,9 +1016,11 @@ void server_pump(mt_server* S) {
     // ---- completed on the device: deliver the results -------------------------
     finished_now.clear();
     uint64_t finished_ops = 0;
+    const uint64_t seen_ns = published.empty() ? 0 : now_ns(S->t0);
     for (size_t k = 0; !rc && k < published.size();) {
       const uint32_t slot = published[k];
       if (__atomic_load_n(&S->done[slot], __ATOMIC_ACQUIRE)) {
+        S->slots[slot].done_ns = seen_ns;
         finished_now.push_back(slot);
         finished_ops += S->slots[slot].n;
         published[k] = published.back();
@@ -1023,6 +1034,7 @@ void server_pump(mt_server* S) {
       if (finished_ops >= kPoolMinOps) S->pool.run(finished_now.size(), deliver);
       else for (size_t k = 0; k < finished_now.size(); ++k) deliver(k);
       const uint64_t now = now_ns(S->t0);
+      uint64_t sq = 0, su = 0, sd = 0, sl = 0, mx = 0;
       for (uint32_t slot : finished_now) {
         srv_request& q = S->slots[slot];
         q.stage = SRV_DONE;
@@ -1031,7 +1043,19 @@ void server_pump(mt_server* S) {
         const uint32_t rec = (uint32_t)(q.ticket % S->L);
         S->rec_latency[rec].store(now - q.submit_ns, std::memory_order_relaxed);
         S->rec_done[rec].store(1u, std::memory_order_release);
+        sq += q.admit_ns - std::min(q.admit_ns, q.submit_ns);
+        su += q.publish_ns - q.admit_ns;
+        sd += q.done_ns - q.publish_ns;
+        sl += now - q.done_ns;
+        mx = std::max(mx, now - q.submit_ns);
       }
+      S->st_queued.fetch_add(sq, std::memory_order_relaxed);
+      S->st_upload.fetch_add(su, std::memory_order_relaxed);
+      S->st_device.fetch_add(sd, std::memory_order_relaxed);
+      S->st_deliver.fetch_add(sl, std::memory_order_relaxed);
+      S->st_ops.fetch_add(finished_ops, std::memory_order_relaxed);
+      if (mx > S->st_max.load(std::memory_order_relaxed)) S->st_max.store(mx, std::memory_order_relaxed);
+      S->st_requests.fetch_add(finished_now.size(), std::memory_order_release);
       progress = true;
     }
     while (!fifo.empty() && S->slots[fifo.front()].stage == SRV_DONE) {
@@ -1222,6 +1246,19 @@ extern "C" int mt_server_poll(mt_server* S, uint64_t ticket, int* done, uint64_t
   return MT_OK;
 }
 
+extern "C" int mt_server_stats(mt_server* S, mt_server_stats_t* out) {
+  if (!S || !out) return MT_ERR_INVALID_ARG;
+  *out = mt_server_stats_t{};
+  out->requests = S->st_requests.load(std::memory_order_acquire);
+  out->ops = S->st_ops.load(std::memory_order_relaxed);
+  out->queued_ns = S->st_queued.load(std::memory_order_relaxed);
+  out->upload_ns = S->st_upload.load(std::memory_order_relaxed);
+  out->device_ns = S->st_device.load(std::memory_order_relaxed);
+  out->deliver_ns = S->st_deliver.load(std::memory_order_relaxed);
+  out->max_latency_ns = S->st_max.load(std::memory_order_relaxed);
+  return MT_OK;
+}
+
 extern "C" int mt_server_stop(mt_server* S) {
   if (!S) return MT_ERR_INVALID_ARG;
   // Serve what is queued; bound the wait, then end the loop regardless.
@@ -1314,6 +1351,8 @@ int serve_online(mt_masstree* t, const mt_serve_plan* plan, uint64_t* latency_ns
   }
   submit_end.store(true, std::memory_order_release);
   poller.join();
+  mt_server_stats_t sst{};
+  mt_server_stats(S, &sst);
   const int stop_rc = mt_server_stop(S);
   uint64_t ops_done = 0, end = 0, done_req = 0;
   for (uint32_t r = 0; r < nreq; ++r) {
@@ -1329,6 +1368,10 @@ int serve_online(mt_masstree* t, const mt_serve_plan* plan, uint64_t* latency_ns
     stats->requests_done = done_req;
     stats->ops_done = ops_done;
     stats->admission_waits = 0;
+    stats->stage_ns[0] = sst.queued_ns;
+    stats->stage_ns[1] = sst.upload_ns;
+    stats->stage_ns[2] = sst.device_ns;
+    stats->stage_ns[3] = sst.deliver_ns;
   }
   if (!rc && poll_fail) rc = MT_ERR_LOCK_TIMEOUT;
   return rc ? rc : stop_rc;

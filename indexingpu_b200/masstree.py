@@ -235,7 +235,9 @@ class GpuMasstree:
         st = _lib.MtServeStats()
         rc = self._lib.mt_serve(self._h, ctypes.byref(plan), lat.ctypes.data, ctypes.byref(st))
         self._check(rc, "mt_serve")
-        return lat, {f: getattr(st, f) for f, _ in _lib.MtServeStats._fields_}
+        out = {f: getattr(st, f) for f, _ in _lib.MtServeStats._fields_ if f != "stage_ns"}
+        out["stage_ns"] = dict(zip(("queued", "upload", "device", "deliver"), (int(x) for x in st.stage_ns)))
+        return lat, out
 
     # -- status ---------------------------------------------------------------------
     def sync(self, stream=0):
@@ -295,6 +297,14 @@ class MasstreeServer:
         if rc != 0:
             raise MasstreeError(rc, "mt_server_poll")
         return bool(d.value), int(lat.value)
+
+    def stats(self):
+        """Stage sums of the requests completed so far (mt_server_stats_t)."""
+        st = _lib.MtServerStats()
+        rc = self._lib.mt_server_stats(self._h, ctypes.byref(st))
+        if rc != 0:
+            raise MasstreeError(rc, "mt_server_stats")
+        return {f: int(getattr(st, f)) for f, _ in _lib.MtServerStats._fields_ if f != "reserved"}
 
     def stop(self):
         if self._h:

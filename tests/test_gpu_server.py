@@ -84,6 +84,13 @@ def _serve_online(torch, g, st, alone, **cfg):
                     time.sleep(0)
                 wait(r)
             th.join()
+        # Stage sums: every request counted once, each stage's sum within the
+        # sum of the requests' latencies.
+        sst = srv.stats()
+        assert sst["requests"] == n_req and sst["ops"] == int(nops.sum()), sst
+        stages = sst["queued_ns"] + sst["upload_ns"] + sst["device_ns"] + sst["deliver_ns"]
+        assert 0 < stages <= int(lat.sum()) + n_req * 1000, (sst, int(lat.sum()))
+        assert sst["max_latency_ns"] >= int(lat.max()), (sst, int(lat.max()))
     finally:
         srv.stop()
     return vals.numpy(), vlens.numpy(), res.numpy().astype(np.uint8), lat
@@ -166,6 +173,7 @@ def test_online_replay_of_a_timed_stream():
         lat, stats = g.t.serve(h["types"], h["keys"], MAXK, h["lens"], h["vals"], MAXV, h["vlens"], res,
                                st["first"], st["nops"], st["arrival_ns"], online=True)
         assert stats["requests_done"] == 400 and (lat > 0).all()
+        assert 0 < sum(stats["stage_ns"].values()) <= int(lat.sum()) + 400 * 1000, stats
         _check(st, (h["vals"].numpy(), h["vlens"].numpy(), res.numpy().astype(np.uint8), lat), exp)
         same_state(g, o, MAXK, MAXV)
     finally:
