@@ -929,6 +929,25 @@ MT_DEV uint32_t coop_scan(const tile<T>& t, const tree_view& tv, const uint32_t*
   return c;
 }
 
+// Ask L2 for the lines a scan reads next in border node nd: the chain (or
+// child layer root) of every entry from `start` on, and the right sibling.
+// Each lane handles the entries whose value words it holds, so nothing is
+// exchanged and no register stays busy: the scan still reads the lines one
+// entry at a time, but from L2 instead of DRAM.
+template <int T>
+MT_DEV void prefetch_scan_lines(const tile<T>& t, const pool_view& p, const node<T>& nd, uint32_t start) {
+  const uint32_t n = nd.count();
+#pragma unroll
+  for (int k = 0; k < node<T>::W; ++k) {
+    const uint32_t g = t.rank * node<T>::W + (uint32_t)k;
+    if ((g & 1u) == 0u || g >= 2u * (uint32_t)kMaxEntries) continue;
+    const uint32_t e = g >> 1;
+    if (e < start || e >= n || ks_get(nd.ks, e) == KS_VALUE || !p.valid(nd.w[k])) continue;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p.addr(nd.w[k])));
+  }
+  if (t.leader() && nd.has_sib() && p.valid(nd.sib)) asm volatile("prefetch.global.L2 [%0];" ::"l"(p.addr(nd.sib)));
+}
+
 template <int T, bool CONCURRENT>
 MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint32_t* lower, uint32_t llen,
                                bool use_upper, const uint32_t* upper, uint32_t ulen, uint32_t max_count,
@@ -954,6 +973,7 @@ MT_DEV uint32_t coop_scan_walk(const tile<T>& t, const tree_view& tv, const uint
     // Walk entries [start, count) of the border node nd at `layer`.
     bool descended = false;
     const uint32_t n = nd.count();
+    prefetch_scan_lines(t, p, nd, start);
     for (uint32_t e = start; e < n; ++e) {
       const uint32_t s = nd.key_at(t, e);
       const uint32_t st = ks_get(nd.ks, e);
