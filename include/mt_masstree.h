@@ -146,9 +146,11 @@ int mt_find(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, co
 
 /* Reference gpu_masstree::insert (gpu_masstree.hpp:101-115).  results may be
  * NULL (the reference has none); else results[i] = inserted (or updated).
- * The first insert of at least 65,536 keys into a tree that holds nothing
+ * An insert of at least 1,024 keys into a tree that holds nothing
  * bulk-builds the tree's first layer (same results and contents); that call
- * waits for the device and allocates temporary scratch. */
+ * waits for the device and allocates temporary scratch, and so does the
+ * emptiness check of every insert of 1,024+ keys until one finds keys in the
+ * tree. */
 int mt_insert(mt_masstree* tree, const uint32_t* keys, uint32_t max_key_length, const uint32_t* key_lengths,
               const uint32_t* values, uint32_t max_value_length, const uint32_t* value_lengths,
               uint32_t num_keys, bool* results, uint32_t flags, void* stream);

@@ -1,25 +1,37 @@
-// Bulk build of a new tree's first layer (the first large insert into a tree
-// that holds nothing yet).
+// Bulk build of a new tree's first layer (an insert into a tree that holds
+// nothing yet).
 //
 // Inserted one by one, such a batch starts every tile on the single root node,
-// and node splits serialise there until the tree has thousands of leaves.  The
-// reference inserts one by one as well (include/gpu_masstree.hpp:101-115).  Here
-// the batch is ordered by its first slice on the device; every key whose first
-// slice no other key of the batch shares becomes a layer-0 entry directly (its
-// value, or a suffix chain of its key rest and value, built by one tile each),
-// the entries are packed into border nodes in key order, and the interior
-// levels are written bottom-up, the top node into the root slab.  The other
-// keys (a first slice shared with another key, invalid lengths) are then
-// inserted by the ordinary insert kernel, which also reports their results.
-// Nodes are packed to kBulkFill entries so that later inserts find room.
+// and node splits serialise there until the tree has thousands of leaves (a
+// few thousand keys took milliseconds).  The reference inserts one by one as
+// well (include/gpu_masstree.hpp:101-115).  Here the batch is sorted on the
+// device by (first slice, whether the key continues past it), the key-order
+// position of a layer-0 entry (a key ending at a slice sorts before one that
+// continues with it).  Each run of one such position becomes one layer-0
+// entry:
+//   * a run of one key: the key's entry itself (its value, or a suffix chain of
+//     its key rest and value), built by one tile each;
+//   * a run of keys that continue past one first slice: a LINK entry to a new,
+//     empty layer-1 root, and the keys are inserted afterwards;
+//   * a run of keys ending at one first slice (the same key more than once):
+//     no entry, the keys are inserted afterwards (one of them wins).
+// The entries are packed into border nodes in key order, and the interior
+// levels are written bottom-up, the top node into the root slab.  The keys
+// left over (and invalid ones) then go through the ordinary insert kernel,
+// which also reports their results: they meet in their own layer-1 roots, one
+// per shared first slice, instead of all in the root.  Nodes are packed to
+// kBulkFill entries so that later inserts find room.
 #include <algorithm>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "mt_internal.cuh"
 
 namespace mtb {
 
-constexpr uint32_t kBuckets = 1u << 16;  // ordered by the top 16 bits of the first slice, then sorted
-constexpr uint32_t kBulkFill = 10;       // entries per built node (of kMaxEntries)
+constexpr uint32_t kBulkFill = 10;                    // entries per built node (of kMaxEntries)
+constexpr unsigned long long kBulkInvalid = 1ull << 33;  // sort key of an invalid request (after all valid ones)
+constexpr int kBulkSortBits = 34;
 
 struct bulk_view {
   const uint32_t* keys;
@@ -28,14 +40,12 @@ struct bulk_view {
   const uint32_t* vlens;
   bool* results;
   uint32_t max_key_length, max_value_length, n;
-  uint32_t* counts;          // [kBuckets] keys per bucket, then fill cursors
-  uint32_t* offsets;         // [kBuckets] first position of every bucket
-  uint32_t* ctl;             // [0] valid keys, [1] largest bucket, [2] rest count, [3] unique count,
-                             // [4] buckets holding keys
-  unsigned long long* order; // [n] (first slice << 32 | request) in key order
-  uint32_t* rest;            // [n] requests left to the ordinary insert
-  uint32_t* block_uniques;   // [blocks of the classify pass] unique keys per block, then their offsets
-  uint32_t* e_slice;         // [n] per unique entry: slice, value word, key state, request
+  uint32_t* ctl;                  // [0] valid keys, [2] rest count, [3] entries
+  unsigned long long* sort_key;   // [n] (first slice << 1 | continues) in key order (after the sort)
+  uint32_t* sort_req;             // [n] the request at each sorted position
+  uint32_t* rest;                 // [n] requests left to the ordinary insert
+  uint32_t* block_entries;        // [blocks of the classify pass] entries per block, then their offsets
+  uint32_t* e_slice;              // [n] per entry: slice, value word, key state, request (kInvalid: LINK)
   uint32_t* e_val;
   uint32_t* e_state;
   uint32_t* e_src;
@@ -47,103 +57,67 @@ MT_DEV bool bulk_valid(const bulk_view& b, uint32_t i) {
   return kl >= 1u && kl <= b.max_key_length && vl <= b.max_value_length && kl <= kMaxLen16 && vl <= kMaxLen16;
 }
 
-__global__ void bulk_count_kernel(bulk_view b) {
+// Sort keys of all requests; invalid requests go to the rest at once.
+__global__ void bulk_keys_kernel(bulk_view b, unsigned long long* key_out, uint32_t* req_out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x) {
-    if (!bulk_valid(b, i)) {
+    unsigned long long k = kBulkInvalid;
+    if (bulk_valid(b, i)) {
+      const uint32_t kl = b.klens ? b.klens[i] : b.max_key_length;
+      k = ((unsigned long long)b.keys[(size_t)i * b.max_key_length] << 1) | (kl > 1u ? 1ull : 0ull);
+      atomicAdd(&b.ctl[0], 1u);
+    } else {
       b.rest[atomicAdd(&b.ctl[2], 1u)] = i;
-      continue;
     }
-    const uint32_t bucket = b.keys[(size_t)i * b.max_key_length] >> 16;
-    const uint32_t c = atomicAdd(&b.counts[bucket], 1u) + 1u;
-    if (c == 1u) atomicAdd(&b.ctl[4], 1u);
-    atomicMax(&b.ctl[1], c);
-    atomicAdd(&b.ctl[0], 1u);
+    key_out[i] = k;
+    req_out[i] = i;
   }
 }
 
-// Exclusive prefix sums of the bucket sizes (one block of 1024 threads).
-__global__ void bulk_scan_kernel(bulk_view b) {
-  __shared__ uint32_t part[1024];
-  constexpr uint32_t per = kBuckets / 1024u;
-  const uint32_t base = threadIdx.x * per;
-  uint32_t s = 0;
-  for (uint32_t k = 0; k < per; ++k) s += b.counts[base + k];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (uint32_t d = 1; d < 1024u; d <<= 1) {
-    const uint32_t v = threadIdx.x >= d ? part[threadIdx.x - d] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  uint32_t run = part[threadIdx.x] - s;
-  for (uint32_t k = 0; k < per; ++k) {
-    const uint32_t c = b.counts[base + k];
-    b.offsets[base + k] = run;
-    b.counts[base + k] = run;  // fill cursor
-    run += c;
-  }
+// What sorted position j (of m valid ones) becomes: an entry of its own
+// (alone in its run), the LINK entry of a run of continuing keys (its first
+// position), and / or a request for the ordinary insert (every position of a
+// run of two or more).
+MT_DEV void bulk_position(const bulk_view& b, uint32_t j, uint32_t m, bool& entry, bool& to_rest) {
+  const unsigned long long k = b.sort_key[j];
+  const bool first = j == 0 || b.sort_key[j - 1] != k;
+  const bool last = j + 1 >= m || b.sort_key[j + 1] != k;
+  const bool alone = first && last;
+  entry = alone || (first && (k & 1ull) != 0ull);
+  to_rest = !alone;
 }
 
-__global__ void bulk_scatter_kernel(bulk_view b) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.n; i += gridDim.x * blockDim.x) {
-    if (!bulk_valid(b, i)) continue;
-    const uint32_t s0 = b.keys[(size_t)i * b.max_key_length];
-    const uint32_t pos = atomicAdd(&b.counts[s0 >> 16], 1u);
-    b.order[pos] = ((unsigned long long)s0 << 32) | i;
-  }
-}
-
-// Sort inside every bucket (insertion sort; buckets are small, the host checks).
-__global__ void bulk_sort_kernel(bulk_view b) {
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < kBuckets; k += gridDim.x * blockDim.x) {
-    const uint32_t lo = b.offsets[k], hi = b.counts[k];  // counts: end of the bucket after the scatter
-    for (uint32_t x = lo + 1; x < hi; ++x) {
-      const unsigned long long v = b.order[x];
-      uint32_t y = x;
-      while (y > lo && b.order[y - 1] > v) {
-        b.order[y] = b.order[y - 1];
-        --y;
-      }
-      b.order[y] = v;
-    }
-  }
-}
-
-// Whether position j of the ordered keys holds a first slice no other key has.
-MT_DEV bool bulk_unique(const bulk_view& b, uint32_t j, uint32_t m) {
-  const uint32_t s = (uint32_t)(b.order[j] >> 32);
-  return (j == 0 || (uint32_t)(b.order[j - 1] >> 32) != s) && (j + 1 >= m || (uint32_t)(b.order[j + 1] >> 32) != s);
-}
-
-// Pass 1: unique keys per block of 256 positions; the others go to the rest.
-__global__ void bulk_classify_kernel(bulk_view b, uint32_t m) {
+// Pass 1: entries per block of 256 positions; the others go to the rest.
+__global__ void bulk_classify_kernel(bulk_view b) {
+  const uint32_t m = b.ctl[0];
   const uint32_t j = blockIdx.x * 256u + threadIdx.x;
-  const bool u = j < m && bulk_unique(b, j, m);
-  if (j < m && !u) b.rest[atomicAdd(&b.ctl[2], 1u)] = (uint32_t)b.order[j];
-  const uint32_t c = __syncthreads_count(u);
-  if (threadIdx.x == 0) b.block_uniques[blockIdx.x] = c;
+  bool entry = false, to_rest = false;
+  if (j < m) bulk_position(b, j, m, entry, to_rest);
+  if (to_rest) b.rest[atomicAdd(&b.ctl[2], 1u)] = b.sort_req[j];
+  const uint32_t c = __syncthreads_count(entry);
+  if (threadIdx.x == 0) b.block_entries[blockIdx.x] = c;
 }
 
-// Exclusive sums of the per-block counts (one block); ctl[3] = total.
+// Exclusive sums of the per-block counts (one thread); ctl[3] = total.
 __global__ void bulk_block_scan_kernel(bulk_view b, uint32_t nblocks) {
   if (threadIdx.x != 0) return;
   uint32_t run = 0;
   for (uint32_t k = 0; k < nblocks; ++k) {
-    const uint32_t c = b.block_uniques[k];
-    b.block_uniques[k] = run;
+    const uint32_t c = b.block_entries[k];
+    b.block_entries[k] = run;
     run += c;
   }
   b.ctl[3] = run;
 }
 
-// Pass 2: unique keys, in key order, to the entry arrays.
-__global__ void bulk_compact_kernel(bulk_view b, uint32_t m) {
+// Pass 2: the entries, in key order, to the entry arrays.
+__global__ void bulk_compact_kernel(bulk_view b) {
   __shared__ uint32_t warp_base[8];
+  const uint32_t m = b.ctl[0];
   const uint32_t j = blockIdx.x * 256u + threadIdx.x;
-  const bool u = j < m && bulk_unique(b, j, m);
+  bool entry = false, to_rest = false;
+  if (j < m) bulk_position(b, j, m, entry, to_rest);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t bal = __ballot_sync(0xFFFFFFFFu, u);
+  const uint32_t bal = __ballot_sync(0xFFFFFFFFu, entry);
   if (lane == 0) warp_base[warp] = __popc(bal);
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -155,15 +129,16 @@ __global__ void bulk_compact_kernel(bulk_view b, uint32_t m) {
     }
   }
   __syncthreads();
-  if (u) {
-    const uint32_t pos = b.block_uniques[blockIdx.x] + warp_base[warp] + __popc(bal & ((1u << lane) - 1u));
-    b.e_slice[pos] = (uint32_t)(b.order[j] >> 32);
-    b.e_src[pos] = (uint32_t)b.order[j];
+  if (entry) {
+    const uint32_t pos = b.block_entries[blockIdx.x] + warp_base[warp] + __popc(bal & ((1u << lane) - 1u));
+    b.e_slice[pos] = (uint32_t)(b.sort_key[j] >> 1);
+    b.e_src[pos] = to_rest ? kInvalid : b.sort_req[j];
   }
 }
 
-// The value word and key state of every unique entry (a 32-lane tile each:
-// chains are written cooperatively); its request reports success.
+// The value word and key state of every entry (a 32-lane tile each: chains
+// are written cooperatively); the request of a key's own entry reports
+// success.
 __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) bulk_entry_kernel(tree_view tv, bulk_view b,
                                                                                   uint32_t nu) {
   tile<32> t;
@@ -172,9 +147,24 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) bulk_entry_kerne
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / 32u;
   cache.init(tv.pool, tile_id);
   const pool_view& p = tv.pool;
+  nu = min(nu, b.ctl[3]);  // entries found by the compaction (nu: capacity)
   for (uint32_t u = tile_id; u < nu; u += num_tiles) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(p)), 0)) break;
     const uint32_t i = b.e_src[u];
+    if (i == kInvalid) {
+      // A LINK entry: a new, empty root for the layer below this first slice.
+      const uint32_t r = cache.allocate(t, p);
+      if (r != kInvalid) {
+        node<32> nd;
+        make_layer_root(t, nd, r);
+        publish_new(t, p, nd);
+      }
+      if (t.leader()) {
+        b.e_val[u] = r;
+        b.e_state[u] = r != kInvalid ? KS_LINK : 0xFFFFFFFFu;
+      }
+      continue;
+    }
     const uint32_t klen = b.klens ? b.klens[i] : b.max_key_length;
     const uint32_t vlen = b.vlens ? b.vlens[i] : b.max_value_length;
     const uint32_t* key = b.keys + (size_t)i * b.max_key_length;
@@ -228,10 +218,17 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) bulk_node_kernel
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / 32u;
   const pool_view& p = tv.pool;
+  // Node k takes entries [k*F, (k+1)*F), each bound moved one up when it
+  // would part the two entries of one slice (a key ending there and one
+  // continuing), which must share a node: lookups of the slice go to the
+  // node whose high key it is.
+  auto bound = [&](uint32_t x) {
+    return (x == 0u || x >= count) ? min(x, count) : x + (key[x - 1u] == key[x] ? 1u : 0u);
+  };
   for (uint32_t k = tile_id; k < nodes; k += num_tiles) {
-    const uint32_t first = k * kBulkFill;
-    const uint32_t cnt = min(kBulkFill, count - first);
+    const uint32_t first = bound(k * kBulkFill);
     const bool last = k + 1u == nodes;
+    const uint32_t cnt = (last ? count : bound((k + 1u) * kBulkFill)) - first;
     node<32> nd;
     nd.idx = ids[k];
     if (!p.valid(nd.idx)) {
@@ -266,12 +263,6 @@ namespace {
 
 int cu(cudaError_t e) { return e == cudaSuccess ? MT_OK : MT_ERR_CUDA; }
 
-template <typename X>
-int dalloc(X** p, size_t n) {
-  return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(X)) == cudaSuccess ? MT_OK
-                                                                                                    : MT_ERR_OOM;
-}
-
 }  // namespace
 
 namespace mtb {
@@ -291,76 +282,79 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
   b.max_value_length = a.max_value_length;
   b.n = n;
   const uint32_t cblocks = (n + 255u) / 256u;
-  int rc = dalloc(&b.counts, kBuckets);
-  if (!rc) rc = dalloc(&b.offsets, kBuckets);
-  if (!rc) rc = dalloc(&b.ctl, 8);
-  if (!rc) rc = dalloc(&b.order, n);
-  if (!rc) rc = dalloc(&b.rest, n);
-  if (!rc) rc = dalloc(&b.block_uniques, cblocks);
-  if (!rc) rc = dalloc(&b.e_slice, n);
-  if (!rc) rc = dalloc(&b.e_val, n);
-  if (!rc) rc = dalloc(&b.e_state, n);
-  if (!rc) rc = dalloc(&b.e_src, n);
-  uint32_t* ids = nullptr;
-  uint32_t* highs[2] = {nullptr, nullptr};
   const uint32_t max_nodes = n / kBulkFill + 2u;
-  if (!rc) rc = dalloc(&ids, max_nodes);
-  if (!rc) rc = dalloc(&highs[0], max_nodes);
-  if (!rc) rc = dalloc(&highs[1], max_nodes);
-  uint32_t* ids2 = nullptr;
-  if (!rc) rc = dalloc(&ids2, max_nodes);
-  auto release = [&] {
-    for (void* q : {(void*)b.counts, (void*)b.offsets, (void*)b.ctl, (void*)b.order, (void*)b.rest,
-                    (void*)b.block_uniques, (void*)b.e_slice, (void*)b.e_val, (void*)b.e_state, (void*)b.e_src,
-                    (void*)ids, (void*)ids2, (void*)highs[0], (void*)highs[1]})
-      if (q) cudaFree(q);
-  };
-  if (rc) {
+  // One allocation for all scratch: the sort's input and output, its own
+  // temporary storage, and the arrays of the build.
+  size_t sort_bytes = 0;
+  if (cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (unsigned long long*)nullptr,
+                                      (unsigned long long*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0,
+                                      kBulkSortBits, s) != cudaSuccess)
+    return kBulkDeclined;
+  auto up = [](size_t x) { return (x + 255u) & ~size_t(255); };
+  const size_t n64 = up((size_t)n * 8u), n32 = up((size_t)n * 4u), nodes32 = up((size_t)max_nodes * 4u);
+  const size_t total = 2 * n64 + 2 * n32 + up(sort_bytes) + up(8 * 4u) + 5 * n32 + up((size_t)cblocks * 4u) +
+                       4 * nodes32;
+  char* mem = nullptr;
+  if (cudaMalloc(&mem, total) != cudaSuccess) {
     // No room for the scratch beside the slab pool: the ordinary insert needs
     // none.  Clear the failed allocation's error so later launch checks do
     // not report it.
     cudaGetLastError();
-    release();
     return kBulkDeclined;
   }
+  char* q = mem;
+  auto carve = [&](size_t bytes) {
+    char* r = q;
+    q += bytes;
+    return r;
+  };
+  auto* key_in = reinterpret_cast<unsigned long long*>(carve(n64));
+  b.sort_key = reinterpret_cast<unsigned long long*>(carve(n64));
+  auto* req_in = reinterpret_cast<uint32_t*>(carve(n32));
+  b.sort_req = reinterpret_cast<uint32_t*>(carve(n32));
+  void* sort_tmp = carve(up(sort_bytes));
+  b.ctl = reinterpret_cast<uint32_t*>(carve(up(8 * 4u)));
+  b.rest = reinterpret_cast<uint32_t*>(carve(n32));
+  b.e_slice = reinterpret_cast<uint32_t*>(carve(n32));
+  b.e_val = reinterpret_cast<uint32_t*>(carve(n32));
+  b.e_state = reinterpret_cast<uint32_t*>(carve(n32));
+  b.e_src = reinterpret_cast<uint32_t*>(carve(n32));
+  b.block_entries = reinterpret_cast<uint32_t*>(carve(up((size_t)cblocks * 4u)));
+  uint32_t* ids = reinterpret_cast<uint32_t*>(carve(nodes32));
+  uint32_t* ids2 = reinterpret_cast<uint32_t*>(carve(nodes32));
+  uint32_t* highs[2] = {reinterpret_cast<uint32_t*>(carve(nodes32)), reinterpret_cast<uint32_t*>(carve(nodes32))};
+
   uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t err = 0;
   const int grid = std::max(1, t->sms * 8);
-  if (!rc) rc = cu(cudaMemsetAsync(b.counts, 0, kBuckets * sizeof(uint32_t), s));
-  if (!rc) rc = cu(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(uint32_t), s));
+  int rc = cu(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(uint32_t), s));
   if (!rc) {
-    bulk_count_kernel<<<grid, 256, 0, s>>>(b);
+    bulk_keys_kernel<<<std::min<uint32_t>(grid, cblocks), 256, 0, s>>>(b, key_in, req_in);
+    rc = cu(cudaGetLastError());
+  }
+  size_t sb = sort_bytes;
+  if (!rc)
+    rc = cu(cub::DeviceRadixSort::SortPairs(sort_tmp, sb, key_in, b.sort_key, req_in, b.sort_req, (int)n, 0,
+                                            kBulkSortBits, s));
+  if (!rc) {
+    bulk_classify_kernel<<<cblocks, 256, 0, s>>>(b);
+    bulk_block_scan_kernel<<<1, 32, 0, s>>>(b, cblocks);
+    bulk_compact_kernel<<<cblocks, 256, 0, s>>>(b);
+    rc = cu(cudaGetLastError());
+  }
+  // Every entry's value word and key state (capacity: all positions), then
+  // the counts and the error word.
+  if (!rc) {
+    bulk_entry_kernel<<<grid, kBlock, 0, s>>>(t->tv, b, n);
     rc = cu(cudaGetLastError());
   }
   if (!rc) rc = cu(cudaMemcpyAsync(h, b.ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  if (!rc) rc = cu(cudaMemcpyAsync(&err, t->tv.pool.err, sizeof(err), cudaMemcpyDeviceToHost, s));
   if (!rc) rc = cu(cudaStreamSynchronize(s));
-  const uint32_t m = h[0];
-  // Decline when one bucket is large, or the keys crowd into few buckets
-  // (first slices shared by many keys: little to build, and the in-bucket
-  // sort would be slow), or fewer than half the keys are valid.
-  bool declined = !rc && (h[1] > 2048u || h[4] < std::min<uint32_t>(m, kBuckets) / 64u || m < n / 2u);
-  if (!rc && !declined) {
-    bulk_scan_kernel<<<1, 1024, 0, s>>>(b);
-    bulk_scatter_kernel<<<grid, 256, 0, s>>>(b);
-    bulk_sort_kernel<<<(kBuckets + 255u) / 256u, 256, 0, s>>>(b);
-    const uint32_t mblocks = std::max(1u, (m + 255u) / 256u);
-    bulk_classify_kernel<<<mblocks, 256, 0, s>>>(b, m);
-    bulk_block_scan_kernel<<<1, 32, 0, s>>>(b, mblocks);
-    bulk_compact_kernel<<<mblocks, 256, 0, s>>>(b, m);
-    rc = cu(cudaGetLastError());
-    if (!rc) rc = cu(cudaMemcpyAsync(h, b.ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
-    if (!rc) rc = cu(cudaStreamSynchronize(s));
-  }
+  if (!rc && err != 0u) rc = (int)err;
   const uint32_t nu = h[3];
-  if (!rc && !declined && nu == 0u) declined = true;
-  if (!rc && !declined) {
-    // Entries, then (unless building them failed: pool exhausted) the levels
-    // bottom-up.
-    bulk_entry_kernel<<<grid, kBlock, 0, s>>>(t->tv, b, nu);
-    rc = cu(cudaGetLastError());
-    uint32_t err = 0;
-    if (!rc) rc = cu(cudaMemcpyAsync(&err, t->tv.pool.err, sizeof(err), cudaMemcpyDeviceToHost, s));
-    if (!rc) rc = cu(cudaStreamSynchronize(s));
-    if (!rc && err != 0u) rc = (int)err;
+  if (!rc && nu > 0u) {
+    // The levels bottom-up.
     uint32_t count = nu;
     const uint32_t* key = b.e_slice;
     const uint32_t* val = b.e_val;
@@ -384,25 +378,18 @@ int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStrea
       hi ^= 1;
       std::swap(cur_ids, next_ids);
     }
-    if (!rc) rc = cu(cudaStreamSynchronize(s));
   }
-  if (!rc && !declined) {
+  if (!rc && h[2] > 0u) {
     // The rest through the ordinary insert kernel.
-    if (!rc) rc = cu(cudaMemcpyAsync(h, b.ctl, sizeof(h), cudaMemcpyDeviceToHost, s));
-    if (!rc) rc = cu(cudaStreamSynchronize(s));
-    if (!rc && h[2] > 0u) {
-      batch_args r = a;
-      r.index = b.rest;
-      r.n_dev = b.ctl + 2;
-      r.n = h[2];
-      rc = host_launch_insert(t, r, upsert, s);
-      if (!rc) rc = cu(cudaStreamSynchronize(s));
-    }
+    batch_args r = a;
+    r.index = b.rest;
+    r.n_dev = b.ctl + 2;
+    r.n = h[2];
+    rc = host_launch_insert(t, r, upsert, s);
   }
   cudaStreamSynchronize(s);
-  release();
-  if (rc) return rc;
-  return declined ? kBulkDeclined : MT_OK;
+  cudaFree(mem);
+  return rc;
 }
 
 }  // namespace mtb

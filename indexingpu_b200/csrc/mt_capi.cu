@@ -682,10 +682,17 @@ int mt_insert(mt_masstree* t, const uint32_t* keys, uint32_t maxK, const uint32_
   a.results = results; a.max_key_length = maxK; a.max_value_length = maxV; a.n = n;
   cudaStream_t s = (cudaStream_t)stream;
   const bool upsert = (flags & MT_FLAG_UPDATE_IF_EXISTS) != 0;
-  if (n >= kBulkMin && tree_is_empty(t)) {
-    const int rc = host_bulk_insert(t, a, upsert, s);
-    if (rc != kBulkDeclined) return rc;
+  // The emptiness check waits for the device: only until an insert call
+  // finds the tree holding keys (erasing every key later forgoes the build).
+  if (n >= kBulkMin && t->maybe_empty) {
+    const bool empty = tree_is_empty(t);
+    t->maybe_empty = false;
+    if (empty) {
+      const int rc = host_bulk_insert(t, a, upsert, s);
+      if (rc != kBulkDeclined) return rc;
+    }
   }
+  if (n) t->maybe_empty = false;
   return upsert ? launch_batch<OP_UPSERT, true>(t, a, s) : launch_batch<OP_INSERT, true>(t, a, s);
 }
 

@@ -203,6 +203,7 @@ struct mt_masstree {
   uint64_t batches_max_total = 0;
   // Merge log of MT_FLAG_MERGE calls and layer log of
   // MT_FLAG_REMOVE_EMPTY_LAYERS calls (see mt_merge.cu; created on first use).
+  bool maybe_empty = true;  // no insert call has found the tree holding keys yet (bulk build candidate)
   uint32_t* merge_log = nullptr;
   uint32_t* layer_log = nullptr;
 };
@@ -223,7 +224,7 @@ int host_launch_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStr
 // Bulk build of a new tree's first layer (mt_bulk.cu): MT_OK, an error, or
 // kBulkDeclined when the batch does not suit it (insert it as usual).
 constexpr int kBulkDeclined = -1000;
-constexpr uint32_t kBulkMin = 1u << 16;  // smallest insert call that may bulk-build
+constexpr uint32_t kBulkMin = 1u << 10;  // smallest insert call that may bulk-build
 int host_bulk_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s);
 bool host_valid_tile(uint32_t ts);
 }  // namespace mtb

@@ -1,7 +1,9 @@
-"""The first large insert into an empty tree bulk-builds its first layer
-(mt_insert with at least 65,536 keys into a tree that holds nothing).  Results,
-found values and the full ordered contents must equal the oracle's, the tree
-must validate, and it must keep working under ordinary mixed batches."""
+"""An insert of 1,024 keys or more into an empty tree bulk-builds its first
+layer: one entry per key alone at its first slice, a LINK entry to a new layer
+for keys that continue past a shared first slice (those keys are then inserted
+below it).  Results, found values and the full ordered contents must equal the
+oracle's, the tree must validate, and it must keep working under ordinary
+mixed batches."""
 import numpy as np
 import pytest
 
@@ -108,16 +110,58 @@ def test_bulk_built_tree_takes_mixed_batches():
         g.close()
 
 
-def test_c2_batch_declines_the_bulk_build():
-    """Keys that all share first slices with others: nothing to build, every
-    key goes through the ordinary insert."""
-    c2 = wl.C2(n_preload=100000, n_prefixes=64)
-    keys, lens, vals, vlens = c2.keys(np.arange(100000))
+@pytest.mark.parametrize("n", [1024, 3000, 100000])
+def test_c2_batch_builds_links(n):
+    """Keys that share their first slices (64 prefixes of 4 slices): layer 0 is
+    built as 64 LINK entries and every key is inserted below them."""
+    c2 = wl.C2(n_preload=n, n_prefixes=64)
+    keys, lens, vals, vlens = c2.keys(np.arange(n))
     g, o = GpuIndex(tile_size=8, pool_bytes=1 << 30), OracleIndex()
     try:
         np.testing.assert_array_equal(g.insert(keys, lens, vals, vlens), o.insert(keys, lens, vals, vlens))
         ok, nkeys, report = g.t.validate()
         assert ok, report
-        assert nkeys == 100000
+        assert nkeys == n
+        same_state(g, o, c2.maxK, c2.maxV)
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("n_first", [700, 5000])
+def test_bulk_build_keeps_slice_pairs_together(n_first):
+    """First slices that hold both a key ending there and keys continuing past
+    it (two entries of one slice), mixed with slices holding one of the two,
+    so that node bounds fall between such pairs; small batches below the old
+    bulk threshold too.  Every key must be reachable."""
+    rng = np.random.default_rng(n_first)
+    firsts = np.unique(rng.integers(0, 1 << 32, 2 * n_first, dtype=np.uint64).astype(np.uint32))[:n_first]
+    kind = rng.integers(0, 4, n_first)  # 0: ends only, 1: one continuing, 2: both, 3: ends + two continuing
+    rows = []
+    for s, k in zip(firsts, kind):
+        if k in (0, 2, 3):
+            rows.append((s, 0, 1))
+        if k in (1, 2):
+            rows.append((s, int(rng.integers(0, 1 << 32)), 2))
+        if k == 3:
+            rows.append((s, 5, 2))
+            rows.append((s, 6, 2))
+    rows = np.array(rows, dtype=np.uint64)
+    rng.shuffle(rows)
+    keys = rows[:, :2].astype(np.uint32)
+    lens = rows[:, 2].astype(np.uint32)
+    n = len(keys)
+    vlens = rng.integers(1, 4, n).astype(np.uint32)
+    vals = rng.integers(0, 1 << 32, (n, 3), dtype=np.uint64).astype(np.uint32)
+    vals[np.arange(3)[None, :] >= vlens[:, None]] = 0
+    g, o = GpuIndex(tile_size=8, pool_bytes=256 << 20), OracleIndex()
+    try:
+        np.testing.assert_array_equal(g.insert(keys, lens, vals, vlens), o.insert(keys, lens, vals, vlens))
+        ok, nkeys, report = g.t.validate()
+        assert ok, report
+        assert nkeys == n
+        gv, gl = g.find(keys, lens, 3)
+        ov, ol = o.find(keys, lens, 3)
+        assert_found(gv, gl, ov, ol, "finds after a bulk build with slice pairs")
+        same_state(g, o, 2, 3)
     finally:
         g.close()
