@@ -480,11 +480,24 @@ def run_batched(args, tree, c2, stream):
     autotune.apply(tree, best)
     tree.reserve_batches(args.subbatches, total_b)
     side = torch.cuda.Stream()
+    grouped = best["form"] == "grouped"
+    if grouped:
+        # The grouped form sizes its scratch on its first call after the
+        # reserve: one untimed call of a single find that misses (the tree
+        # does not change), outside the capture.
+        one = dict(types=torch.full((1,), wl.REQ_FIND, dtype=torch.uint8, device="cuda"),
+                   keys=torch.zeros((1, MAXK), dtype=torch.uint32, device="cuda"),
+                   lens=torch.full((1,), MAXK, dtype=torch.uint32, device="cuda"),
+                   vals=torch.zeros((1, MAXV), dtype=torch.uint32, device="cuda"),
+                   vlens=torch.zeros(1, dtype=torch.uint32, device="cuda"), results=None, n=1)
+        one_desc = torch.from_numpy(pack_subbatches([one])).cuda()
+        tree.mixed_batches(one_desc, 1, MAXK, MAXV, stream=side, group_by_key=True)
+        tree.sync(side)
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g, stream=side):
         tree.mixed_batches(desc, args.subbatches, MAXK, MAXV, stream=side, bucket_keys=best["bucketing"],
-                           persistent=best["form"] == "persistent")
+                           persistent=best["form"] == "persistent", group_by_key=grouped)
     torch.cuda.synchronize()
     with torch.cuda.stream(side):
         e0.record(side)

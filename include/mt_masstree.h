@@ -60,6 +60,9 @@ enum { MT_REQ_INSERT = 0, MT_REQ_ERASE = 1, MT_REQ_FIND = 2, MT_REQ_UPDATE = 3 }
                                        fold a layer root left with one child into its slab
                                        (reference erase merge levels 2-4; space only, results are
                                        the same) */
+#define MT_FLAG_GROUP_BY_KEY 512u   /* mixed_batches: serve all sub-batches at once, the requests on one key
+                                       resolved in sub-batch order (one tree read and at most one write per
+                                       key that several requests touch) */
 #define MT_FLAG_INPUTS_ON_STREAM 256u /* mixed_batch_host: the uploads wait for the work queued on `stream`
                                        before the call (for host inputs that work produces, e.g. a copy
                                        queued just before); without it the uploads start at once */
@@ -225,10 +228,26 @@ int mt_batches_reserve(mt_masstree* tree, uint32_t max_subbatches, uint64_t max_
  * CUDA graph and replayed after the descriptors' contents change.  Needs
  * mt_batches_reserve; flags may hold MT_FLAG_BUCKET_KEYS and
  * MT_FLAG_PERSISTENT.  Find tile width: mt_set_tile_size (4/8/16/32); write
- * tile width: mt_set_write_tile_size (16 or 32).  The batched counterpart of
- * the reference's per-call mixed_batch (gpu_masstree.hpp:173-191). */
+ * tile width: mt_set_write_tile_size (16 or 32).  With MT_FLAG_GROUP_BY_KEY
+ * all sub-batches are served at once: the requests are sorted by a hash of
+ * their key, each key's requests resolved in sub-batch order (and, inside a
+ * sub-batch, in buffer order) by a segmented scan, the tree read once and
+ * written at most once per key that several requests touch; results and the
+ * final contents are those of one call per sub-batch.  Its first call (and
+ * one after a larger mt_batches_reserve) allocates about 100 bytes per
+ * reserved request plus 4 per reserved request and value slice (outside
+ * graph capture), later calls launch a fixed sequence.  The batched
+ * counterpart of the reference's per-call mixed_batch
+ * (gpu_masstree.hpp:173-191). */
 int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t num_subbatches,
                      uint32_t max_key_length, uint32_t max_value_length, uint32_t flags, void* stream);
+
+/* Diagnostic for MT_FLAG_GROUP_BY_KEY: its sort uses `bits` bits of the key
+ * hash (1..64, default 64).  With fewer, different keys share hashes; the form
+ * finds them when it checks each run key by key and serves such a run one
+ * request after the other (the path tests reach this way).  New in this
+ * library. */
+int mt_set_group_hash_bits(mt_masstree* tree, uint32_t bits);
 
 /* Serving (mt_serve). */
 #define MT_SERVE_SERVED 0u /* device-resident request loop with continuous admission */

@@ -45,6 +45,7 @@ SIGNATURES = {
     "mt_server_poll": (_int, [_p, _u64, ctypes.POINTER(_int), ctypes.POINTER(_u64)]),
     "mt_server_stop": (_int, [_p]),
     "mt_server_stats": (_int, [_p, _p]),
+    "mt_set_group_hash_bits": (_int, [_p, _u32]),
 }
 
 

@@ -1,14 +1,15 @@
 """Autotuner for the batched form (mt_mixed_batches).
 
 Searches the form and launch shape of the call over
-  form (three class kernels per sub-batch on forked streams, or one
-  persistent launch for all sub-batches) x find tile (lanes per find: 4, 8,
-  16, 32) x write tile (lanes per insert, update and erase: 16, 32) x
-  key-length bucketing (off, on),
+  form (three class kernels per sub-batch on forked streams, one persistent
+  launch for all sub-batches, or all sub-batches at once grouped by key) x
+  find tile (lanes per find: 4, 8, 16, 32) x write tile (lanes per insert,
+  update and erase: 16, 32) x key-length bucketing (off, on; the grouped
+  form has no buckets and runs once per tile pair),
 then, for the best of those, blocks per SM 1..8.  This is coordinate descent
-(32 + 8 trials rather than the 256 points of the full grid): blocks per SM only
-trades occupancy against per-warp registers, and is measured with the other
-choices fixed.
+(40 + 8 trials rather than the 384 points of the full grid): blocks per SM
+only trades occupancy against per-warp registers, and is measured with the
+other choices fixed.
 
 Every trial runs on a fresh case from `make_case(i)`: the tree changes under
 every trial (inserts add keys, erases remove them), so replaying one case would
@@ -20,7 +21,7 @@ import time
 FIND_TILES = (4, 8, 16, 32)
 WRITE_TILES = (16, 32)
 BUCKETING = (False, True)
-FORMS = ("forked", "persistent")
+FORMS = ("forked", "persistent", "grouped")
 BLOCKS_PER_SM = tuple(range(1, 9))
 
 
@@ -41,7 +42,7 @@ def time_trial(tree, case, config, stream):
     e0.record(stream)
     tree.mixed_batches(case["descriptors"], case["num_subbatches"], case["max_key_length"],
                        case["max_value_length"], stream=stream, bucket_keys=config["bucketing"],
-                       persistent=config.get("form") == "persistent")
+                       persistent=config.get("form") == "persistent", group_by_key=config.get("form") == "grouped")
     e1.record(stream)
     tree.sync(stream)
     return case["total"] / (e0.elapsed_time(e1) / 1e3) / 1e6
@@ -84,7 +85,7 @@ def tune(tree, make_case, stream=None, find_tiles=FIND_TILES, write_tiles=WRITE_
     for fm in forms:
         for ft in find_tiles:
             for wt in write_tiles:
-                for bk in bucketing:
+                for bk in (bucketing if fm != "grouped" else (False,)):
                     cfg = dict(form=fm, find_tile=ft, write_tile=wt, bucketing=bk, blocks_per_sm=0)
                     m = run(cfg)
                     if m > best_mops:

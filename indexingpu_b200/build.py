@@ -11,7 +11,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libmt_b200.so")
-SOURCES = ["mt_capi.cu", "mt_batches.cu", "mt_serve.cu", "mt_host.cu", "mt_bulk.cu", "mt_merge.cu"]
+SOURCES = ["mt_capi.cu", "mt_batches.cu", "mt_serve.cu", "mt_host.cu", "mt_bulk.cu", "mt_merge.cu",
+           "mt_grouped.cu"]
 HEADERS = ["mt_tile.cuh", "mt_pool.cuh", "mt_node.cuh", "mt_suffix.cuh", "mt_tree.cuh", "mt_internal.cuh"]
 
 NVCC_FLAGS = [

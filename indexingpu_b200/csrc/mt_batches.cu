@@ -30,21 +30,6 @@ namespace cg = cooperative_groups;
 
 namespace mtb {
 
-constexpr uint32_t kCountStride = 8;  // per sub-batch: 3 classes x (front, back), padded
-
-struct batches_view {
-  const mt_subbatch* sub;   // device descriptors
-  uint32_t nsub;
-  uint32_t* offsets;        // [nsub + 1] first request of every sub-batch in the flat order
-  uint32_t* counts;         // [nsub][kCountStride]
-  uint32_t* lists;          // [3][max_total] class index regions
-  uint32_t* status;         // [0] = 1 when the list exceeds the reserved scratch
-  uint32_t max_total;
-  uint32_t max_key_length;
-  uint32_t max_value_length;
-  uint32_t bucket_keys;     // 1: short keys first, long keys last in every class
-};
-
 __global__ void batches_prepare_kernel(batches_view b, pool_view p) {
   if (threadIdx.x == 0) {
     uint64_t acc = 0;
@@ -57,17 +42,6 @@ __global__ void batches_prepare_kernel(batches_view b, pool_view p) {
     if (acc > b.max_total) record_error(p, ERR_INVALID_ARG);
   }
   for (uint32_t i = threadIdx.x; i < b.nsub * kCountStride; i += blockDim.x) b.counts[i] = 0u;
-}
-
-// Sub-batch holding flat request g (binary search over the prefix sums).
-MT_DEV uint32_t find_subbatch(const uint32_t* offsets, uint32_t nsub, uint32_t g) {
-  uint32_t lo = 0, hi = nsub;  // offsets[lo] <= g < offsets[hi]
-  while (hi - lo > 1u) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (offsets[mid] <= g) lo = mid;
-    else hi = mid;
-  }
-  return lo;
 }
 
 __global__ void batches_partition_kernel(batches_view b) {
@@ -291,6 +265,8 @@ extern "C" int mt_mixed_batches(mt_masstree* t, const mt_subbatch* subbatches, u
   int rc = host_launch_reclaim(t, s);
   if (rc) return rc;
   batches_prepare_kernel<<<1, 256, 0, s>>>(b, t->tv.pool);
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
+  if (flags & MT_FLAG_GROUP_BY_KEY) return launch_grouped(t, b, s);
   batches_partition_kernel<<<t->sms * 4, 256, 0, s>>>(b);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
   if (!(flags & MT_FLAG_PERSISTENT)) return launch_forked(t, b, s);

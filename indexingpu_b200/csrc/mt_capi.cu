@@ -602,6 +602,7 @@ int mt_destroy(mt_masstree* t) {
   if (t->frames) cudaFree(t->frames);
   if (t->split_idx) cudaFree(t->split_idx);
   if (t->batches_mem) cudaFree(t->batches_mem);
+  if (t->grouped_mem) cudaFree(t->grouped_mem);
   if (t->merge_log) cudaFree(t->merge_log);
   if (t->layer_log) cudaFree(t->layer_log);
   host_pipe_free(t);

@@ -172,6 +172,37 @@ MT_DEV void serve_requests(const tile<T>& t, const tree_view& tv, slab_cache<T>&
 
 }  // namespace mtb
 
+namespace mtb {
+
+// mt_mixed_batches (mt_batches.cu, mt_grouped.cu): the call's sub-batches and scratch.
+constexpr uint32_t kCountStride = 8;  // per sub-batch: 3 classes x (front, back), padded
+
+struct batches_view {
+  const mt_subbatch* sub;   // device descriptors
+  uint32_t nsub;
+  uint32_t* offsets;        // [nsub + 1] first request of every sub-batch in the flat order
+  uint32_t* counts;         // [nsub][kCountStride]
+  uint32_t* lists;          // [3][max_total] class index regions
+  uint32_t* status;         // [0] = 1 when the list exceeds the reserved scratch
+  uint32_t max_total;
+  uint32_t max_key_length;
+  uint32_t max_value_length;
+  uint32_t bucket_keys;     // 1: short keys first, long keys last in every class
+};
+
+// Sub-batch holding flat request g (binary search over the prefix sums).
+MT_DEV uint32_t find_subbatch(const uint32_t* offsets, uint32_t nsub, uint32_t g) {
+  uint32_t lo = 0, hi = nsub;  // offsets[lo] <= g < offsets[hi]
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (offsets[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+}  // namespace mtb
+
 struct mt_host_pipe;  // staging of mt_mixed_batch_host (mt_host.cu)
 
 struct mt_masstree {
@@ -199,6 +230,10 @@ struct mt_masstree {
   uint32_t last_error_site = 0;  // site of the error the last mt_sync returned
   // Sub-batch scratch of mt_mixed_batches (see mt_batches.cu).
   void* batches_mem = nullptr;
+  void* grouped_mem = nullptr;  // mt_mixed_batches with MT_FLAG_GROUP_BY_KEY (mt_grouped.cu)
+  uint32_t grouped_m = 0, grouped_max_v = 0;
+  size_t grouped_temp = 0;
+  uint32_t group_hash_bits = 64;
   uint32_t batches_max_sub = 0;
   uint64_t batches_max_total = 0;
   // Merge log of MT_FLAG_MERGE calls and layer log of
@@ -220,6 +255,7 @@ int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
 int host_fork(mt_masstree* t, cudaStream_t s);
 int host_join(mt_masstree* t, cudaStream_t s, int rc);
 void host_pipe_free(mt_masstree* t);  // mt_host.cu
+int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s);  // mt_grouped.cu
 int host_launch_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s);
 // Bulk build of a new tree's first layer (mt_bulk.cu): MT_OK, an error, or
 // kBulkDeclined when the batch does not suit it (insert it as usual).

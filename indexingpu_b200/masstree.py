@@ -31,6 +31,7 @@ FLAG_PERSISTENT = 32
 FLAG_MERGE = 64
 FLAG_REMOVE_EMPTY_LAYERS = 128
 FLAG_INPUTS_ON_STREAM = 256
+FLAG_GROUP_BY_KEY = 512
 STATUS = {0: "MT_OK", 1: "MT_ERR_OOM", 2: "MT_ERR_LOCK_TIMEOUT", 3: "MT_ERR_CORRUPT", 4: "MT_ERR_INVALID_ARG",
           5: "MT_ERR_CUDA", 6: "MT_ERR_RETRY_LIMIT", 7: "MT_ERR_KEY_TOO_LONG", 8: "MT_ERR_BATCH_TOO_LARGE"}
 
@@ -110,6 +111,11 @@ class GpuMasstree:
 
     def set_blocks_per_sm(self, blocks_per_sm):
         self._check(self._lib.mt_set_blocks_per_sm(self._h, blocks_per_sm), "mt_set_blocks_per_sm")
+
+    def set_group_hash_bits(self, bits):
+        """Bits of the key hash the grouped form of mixed_batches sorts by
+        (default 64; fewer make different keys share a hash: for tests)."""
+        self._check(self._lib.mt_set_group_hash_bits(self._h, bits), "mt_set_group_hash_bits")
 
     def set_upderase_tile_size(self, tile_size):
         """Lanes per update/erase of mixed batches (0: the write width)."""
@@ -193,12 +199,14 @@ class GpuMasstree:
         self._check(self._lib.mt_batches_reserve(self._h, max_subbatches, max_total_requests), "mt_batches_reserve")
 
     def mixed_batches(self, descriptors, num_subbatches, max_key_length, max_value_length, stream=0,
-                      bucket_keys=False, persistent=False):
+                      bucket_keys=False, persistent=False, group_by_key=False):
         """Serve num_subbatches mixed batches in order (three class kernels per
         sub-batch on forked streams, or one persistent launch for all with
-        persistent=True).  `descriptors` is a device tensor holding
-        mt_subbatch records (see pack_subbatches)."""
-        flags = (FLAG_BUCKET_KEYS if bucket_keys else 0) | (FLAG_PERSISTENT if persistent else 0)
+        persistent=True, or all at once with the requests on each key resolved
+        in sub-batch order with group_by_key=True).  `descriptors` is a device
+        tensor holding mt_subbatch records (see pack_subbatches)."""
+        flags = ((FLAG_BUCKET_KEYS if bucket_keys else 0) | (FLAG_PERSISTENT if persistent else 0) |
+                 (FLAG_GROUP_BY_KEY if group_by_key else 0))
         rc = self._lib.mt_mixed_batches(self._h, _ptr(descriptors), num_subbatches, max_key_length,
                                         max_value_length, flags, _stream(stream))
         self._check(rc, "mt_mixed_batches")

@@ -197,7 +197,8 @@ def test_autotune_small_cases():
                         max_key_length=MAXK, max_value_length=MAXV, keep=(d, res))
 
         best, trials = autotune.tune(t, make_case, blocks_per_sm=(2, 8))
-        assert len(trials) == 32 + 2
+        assert len(trials) == 2 * 16 + 8 + 2  # forked and persistent x 16 shapes, grouped x 8, blocks per SM x 2
+        assert best["form"] in autotune.FORMS
         assert best["find_tile"] in autotune.FIND_TILES and best["write_tile"] in autotune.WRITE_TILES
         assert all(tr["mops"] > 0 for tr in trials)
         ok, _, report = t.validate()
