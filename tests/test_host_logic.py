@@ -30,10 +30,13 @@ def test_autotune_coordinate_descent_picks_the_best():
     best, trials = autotune.tune(None, make_case, trial=trial)
     assert (best["find_tile"], best["write_tile"], best["bucketing"], best["blocks_per_sm"]) == (8, 32, True, 6)
     assert best["form"] == "forked"
-    assert len(trials) == 2 * 4 * 2 * 2 + 8
-    # One warm-up case for all sixteen kernel flavours, then a fresh case per trial.
+    # forked and persistent x 4 find tiles x 2 write tiles x bucketing, grouped
+    # (no buckets) x 4 x 2, then blocks per SM x 8.
+    assert len(trials) == 2 * 4 * 2 * 2 + 4 * 2 + 8
+    assert not any(t["form"] == "grouped" and t["bucketing"] for t in trials)
+    # One warm-up case for all 24 kernel flavours, then a fresh case per trial.
     assert cases == list(range(len(trials) + 1))
-    assert sum(1 for i, _ in seen if i == 0) == 16
+    assert sum(1 for i, _ in seen if i == 0) == 24
     assert best["mops"] == max(t["mops"] for t in trials)
 
 
