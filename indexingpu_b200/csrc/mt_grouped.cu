@@ -102,6 +102,28 @@ MT_DEV greq group_req(const grouped_view& g, uint32_t id) {
   r.vlen = (r.kind == MT_REQ_INSERT || r.kind == MT_REQ_UPDATE) ? r.d->value_lengths[r.i] : 0u;
   return r;
 }
+template <int T>
+MT_DEV greq greq_shfl(const tile<T>& t, const greq& r, int src) {
+  greq q;
+  q.d = reinterpret_cast<const mt_subbatch*>(t.shfl64(reinterpret_cast<uint64_t>(r.d), src));
+  q.i = t.shfl(r.i, src);
+  q.kind = t.shfl(r.kind, src);
+  q.klen = t.shfl(r.klen, src);
+  q.vlen = t.shfl(r.vlen, src);
+  return q;
+}
+// Warp-aggregated append of j to `list` (count at *count) by the lanes where want holds.
+MT_DEV void list_append(bool want, uint32_t* list, uint32_t* count, uint32_t j) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t act = __activemask();
+  const uint32_t bal = __ballot_sync(act, want);
+  if (!bal) return;
+  const uint32_t leader = __ffs(bal) - 1u;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(bal));
+  base = __shfl_sync(act, base, (int)leader);
+  if (want) list[base + __popc(bal & ((1u << lane) - 1u))] = j;
+}
 MT_DEV const uint32_t* greq_key(const grouped_view& g, const greq& r) {
   return r.d->keys + (size_t)r.i * g.b.max_key_length;
 }
@@ -196,15 +218,18 @@ __global__ void group_mark_kernel(grouped_view g) {
 // 4. Work lists: heads of keys touched more than once, writes and finds on
 // keys touched once.
 __global__ void group_list_kernel(grouped_view g) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < g.m; j += gridDim.x * blockDim.x) {
-    if (g.hash[j] >= kGBad || g.pre[j].first != kGNoFirst || (g.flags[j] & 1u)) continue;
-    if (!run_last(g, j)) {
-      g.heads[atomicAdd(&g.counts[0], 1u)] = j;
-    } else if (g.fn[j].a != kGAbsent || g.fn[j].p != kGKeep) {  // not a find
-      g.singles[atomicAdd(&g.counts[1], 1u)] = j;
-    } else {
-      g.finds[atomicAdd(&g.counts[3], 1u)] = j;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < g.m; base += stride) {
+    const uint32_t j = base + threadIdx.x;
+    bool head = false, multi = false, find = false;
+    if (j < g.m && g.hash[j] < kGBad && g.pre[j].first == kGNoFirst && !(g.flags[j] & 1u)) {
+      head = true;
+      multi = !run_last(g, j);
+      find = g.fn[j].a == kGAbsent && g.fn[j].p == kGKeep;
     }
+    list_append(head && multi, g.heads, &g.counts[0], j);
+    list_append(head && !multi && !find, g.singles, &g.counts[1], j);
+    list_append(head && !multi && find, g.finds, &g.counts[3], j);
   }
 }
 
@@ -253,20 +278,32 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) group_head_kerne
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   const uint32_t maxV = g.b.max_value_length;
   const uint32_t nh = g.counts[0], n = nh + g.counts[3];
-  for (uint32_t k = tile_id; k < n; k += num_tiles) {
+  // As in the batch kernels: each lane fetches one entry's request, then the
+  // tile serves the entries one after the other.
+  for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
-    const uint32_t j = k < nh ? g.heads[k] : g.finds[k - nh];
-    const greq r = group_req(g, g.gid[j]);
-    if (k >= nh) {  // a find on a key touched once: served directly
-      const uint32_t vo = coop_find<T, true>(t, tv, greq_key(g, r), r.klen, greq_val(g, r), maxV);
-      if (t.leader()) r.d->value_lengths[r.i] = vo;
-      continue;
+    const uint32_t mine = base + t.rank;
+    uint32_t j = 0;
+    greq rq{};
+    if (mine < n) {
+      j = mine < nh ? g.heads[mine] : g.finds[mine - nh];
+      rq = group_req(g, g.gid[j]);
     }
-    uint32_t vl = 0;
-    const bool found = group_lookup<T>(t, tv, greq_key(g, r), r.klen, g.vals + (size_t)j * maxV, maxV, vl);
-    if (t.leader()) {
-      g.init[j] = found ? vl : kGAbsent;
-      g.act[j] = kGKeep;
+    const uint32_t cnt = min((uint32_t)T, n - base);
+    for (uint32_t q = 0; q < cnt; ++q) {
+      const greq r = greq_shfl(t, rq, (int)q);
+      const uint32_t jj = t.shfl(j, (int)q);
+      if (base + q >= nh) {  // a find on a key touched once: served directly
+        const uint32_t vo = coop_find<T, true>(t, tv, greq_key(g, r), r.klen, greq_val(g, r), maxV);
+        if (t.leader()) r.d->value_lengths[r.i] = vo;
+        continue;
+      }
+      uint32_t vl = 0;
+      const bool found = group_lookup<T>(t, tv, greq_key(g, r), r.klen, g.vals + (size_t)jj * maxV, maxV, vl);
+      if (t.leader()) {
+        g.init[jj] = found ? vl : kGAbsent;
+        g.act[jj] = kGKeep;
+      }
     }
   }
 }
@@ -311,37 +348,55 @@ __global__ void group_result_kernel(grouped_view g) {
   }
 }
 
-// 7. Writes: the requests on keys touched once, and the final write of every
+// 7. Writes: the requests on keys touched once, or the final write of every
 // key touched more than once.
-template <int T>
+// HEADS false: the writes on keys touched once (they need nothing from the
+// other passes and run beside them); true: the final writes.
+template <int T, bool HEADS>
 __global__ void __launch_bounds__(kBlock, MT_WRITE_MIN_BLOCKS_PER_SM) group_write_kernel(tree_view tv, grouped_view g) {
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   slab_cache<T> cache;
   cache.init(tv.pool, tile_id);
-  const uint32_t ns = g.counts[1], n = ns + g.counts[0];
-  for (uint32_t k = tile_id; k < n; k += num_tiles) {
+  const uint32_t n = HEADS ? g.counts[0] : g.counts[1];
+  for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
-    const uint32_t j = k < ns ? g.singles[k] : g.heads[k - ns];
-    const greq r = group_req(g, g.gid[j]);
-    const uint32_t* key = greq_key(g, r);
-    if (k < ns) {
-      int res = RES_FAIL;
-      if (r.kind == MT_REQ_INSERT) res = coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
-      else if (r.kind == MT_REQ_UPDATE) res = coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
-      else res = coop_erase<T>(t, tv, key, r.klen);
-      if (t.leader() && r.d->results) r.d->results[r.i] = res == RES_OK;
-      continue;
+    // Each lane fetches one entry: its request and, for a key touched more
+    // than once, the final write and the request whose value it writes.
+    const uint32_t mine = base + t.rank;
+    greq rq{}, wq{};
+    uint32_t act = kGKeep, init = kGAbsent;
+    if (mine < n) {
+      const uint32_t j = HEADS ? g.heads[mine] : g.singles[mine];
+      rq = group_req(g, g.gid[j]);
+      if (HEADS) {
+        act = g.act[j];
+        init = g.init[j];
+        if (act != kGKeep && act != kGAbsent) wq = group_req(g, act);
+      }
     }
-    const uint32_t a = g.act[j];
-    if (a == kGKeep) continue;
-    if (a == kGAbsent) {
-      coop_erase<T>(t, tv, key, r.klen);
-    } else {
-      const greq w = group_req(g, a);
-      if (g.init[j] == kGAbsent) coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, w), w.vlen);
-      else coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, w), w.vlen);
+    const uint32_t cnt = min((uint32_t)T, n - base);
+    for (uint32_t q = 0; q < cnt; ++q) {
+      const greq r = greq_shfl(t, rq, (int)q);
+      const uint32_t* key = greq_key(g, r);
+      if constexpr (!HEADS) {
+        int res = RES_FAIL;
+        if (r.kind == MT_REQ_INSERT) res = coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
+        else if (r.kind == MT_REQ_UPDATE) res = coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
+        else res = coop_erase<T>(t, tv, key, r.klen);
+        if (t.leader() && r.d->results) r.d->results[r.i] = res == RES_OK;
+      } else {
+        const uint32_t a = t.shfl(act, (int)q);
+        if (a == kGKeep) continue;
+        if (a == kGAbsent) {
+          coop_erase<T>(t, tv, key, r.klen);
+          continue;
+        }
+        const greq w = greq_shfl(t, wq, (int)q);
+        if (t.shfl(init, (int)q) == kGAbsent) coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, w), w.vlen);
+        else coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, w), w.vlen);
+      }
     }
   }
   cache.release(t, tv.pool);
@@ -439,10 +494,14 @@ int launch_find_side(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
 }
 
 template <int TW>
-int launch_write_side(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
-  int rc = launch_tile_kernel<TW>(t, group_write_kernel<TW>, g, s);
+int launch_singles(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
+  int rc = launch_tile_kernel<TW>(t, group_write_kernel<TW, false>, g, s);
   if (!rc) rc = launch_tile_kernel<TW>(t, group_serial_kernel<TW>, g, s);
   return rc;
+}
+template <int TW>
+int launch_heads(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
+  return launch_tile_kernel<TW>(t, group_write_kernel<TW, true>, g, s);
 }
 
 }  // namespace
@@ -497,14 +556,23 @@ int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s) {
   group_mark_kernel<<<grid, 256, 0, s>>>(g);
   group_list_kernel<<<grid, 256, 0, s>>>(g);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
-  switch (t->tile_size) {
-    case 4: rc = launch_find_side<4>(t, g, s); break;
-    case 8: rc = launch_find_side<8>(t, g, s); break;
-    case 16: rc = launch_find_side<16>(t, g, s); break;
-    default: rc = launch_find_side<32>(t, g, s); break;
-  }
+  // Keys touched once (and runs served one by one) on a side stream, beside
+  // the reads, results and final writes of the keys touched more than once:
+  // no key is in both.
+  rc = host_fork(t, s);
   if (rc) return rc;
-  return t->write_tile_size <= 16 ? launch_write_side<16>(t, g, s) : launch_write_side<32>(t, g, s);
+  const bool w16 = t->write_tile_size <= 16;
+  rc = w16 ? launch_singles<16>(t, g, t->side[0]) : launch_singles<32>(t, g, t->side[0]);
+  if (!rc) {
+    switch (t->tile_size) {
+      case 4: rc = launch_find_side<4>(t, g, s); break;
+      case 8: rc = launch_find_side<8>(t, g, s); break;
+      case 16: rc = launch_find_side<16>(t, g, s); break;
+      default: rc = launch_find_side<32>(t, g, s); break;
+    }
+  }
+  if (!rc) rc = w16 ? launch_heads<16>(t, g, s) : launch_heads<32>(t, g, s);
+  return host_join(t, s, rc);
 }
 
 }  // namespace mtb
