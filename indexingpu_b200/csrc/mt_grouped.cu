@@ -79,10 +79,11 @@ struct grouped_view {
   uint32_t* act;             // [m] at a run head: final write (kGKeep none, kGAbsent erase, else insert/update id)
   uint32_t* vals;            // [m][max_value_length] at a run head: the value the tree held
   uint32_t* heads;           // run heads of keys touched more than once (count: counts[0])
-  uint32_t* singles;         // writes on keys touched once (count: counts[1])
+  uint32_t* singles;         // inserts on keys touched once (count: counts[1])
+  uint32_t* singles_ue;      // updates and erases on keys touched once (count: counts[4])
   uint32_t* serial;          // heads of runs served one by one (count: counts[2])
   uint32_t* finds;           // finds on keys touched once (count: counts[3])
-  uint32_t* counts;          // [4], zeroed at the start of the call
+  uint32_t* counts;          // [5], zeroed at the start of the call
   unsigned long long hash_mask;  // bits of the key hash used (mt_set_group_hash_bits)
 };
 
@@ -221,15 +222,18 @@ __global__ void group_list_kernel(grouped_view g) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < g.m; base += stride) {
     const uint32_t j = base + threadIdx.x;
-    bool head = false, multi = false, find = false;
+    bool head = false, multi = false, ins = false, find = false;
     if (j < g.m && g.hash[j] < kGBad && g.pre[j].first == kGNoFirst && !(g.flags[j] & 1u)) {
       head = true;
       multi = !run_last(g, j);
-      find = g.fn[j].a == kGAbsent && g.fn[j].p == kGKeep;
+      ins = g.fn[j].a != kGAbsent;
+      find = !ins && g.fn[j].p == kGKeep;
     }
+    const bool single = head && !multi;
     list_append(head && multi, g.heads, &g.counts[0], j);
-    list_append(head && !multi && !find, g.singles, &g.counts[1], j);
-    list_append(head && !multi && find, g.finds, &g.counts[3], j);
+    list_append(single && ins, g.singles, &g.counts[1], j);
+    list_append(single && !ins && !find, g.singles_ue, &g.counts[4], j);
+    list_append(single && find, g.finds, &g.counts[3], j);
   }
 }
 
@@ -350,16 +354,19 @@ __global__ void group_result_kernel(grouped_view g) {
 
 // 7. Writes: the requests on keys touched once, or the final write of every
 // key touched more than once.
-// HEADS false: the writes on keys touched once (they need nothing from the
-// other passes and run beside them); true: the final writes.
-template <int T, bool HEADS>
+// MODE kGWInsert / kGWUpdErase: the inserts / the updates and erases on keys
+// touched once (they need nothing from the other passes and run beside them,
+// each kernel compiled for its kinds only); kGWHeads: the final writes.
+constexpr int kGWInsert = 0, kGWUpdErase = 1, kGWHeads = 2;
+template <int T, int MODE>
 __global__ void __launch_bounds__(kBlock, MT_WRITE_MIN_BLOCKS_PER_SM) group_write_kernel(tree_view tv, grouped_view g) {
   tile<T> t;
   const uint32_t tile_id = (blockIdx.x * blockDim.x + threadIdx.x) / T;
   const uint32_t num_tiles = (gridDim.x * blockDim.x) / T;
   slab_cache<T> cache;
   cache.init(tv.pool, tile_id);
-  const uint32_t n = HEADS ? g.counts[0] : g.counts[1];
+  constexpr bool HEADS = MODE == kGWHeads;
+  const uint32_t n = HEADS ? g.counts[0] : (MODE == kGWInsert ? g.counts[1] : g.counts[4]);
   for (uint32_t base = tile_id * T; base < n; base += num_tiles * T) {
     if (t.shfl((uint32_t)(t.leader() && fatal_error(tv.pool)), 0)) break;
     // Each lane fetches one entry: its request and, for a key touched more
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(kBlock, MT_WRITE_MIN_BLOCKS_PER_SM) group_writ
     greq rq{}, wq{};
     uint32_t act = kGKeep, init = kGAbsent;
     if (mine < n) {
-      const uint32_t j = HEADS ? g.heads[mine] : g.singles[mine];
+      const uint32_t j = HEADS ? g.heads[mine] : (MODE == kGWInsert ? g.singles[mine] : g.singles_ue[mine]);
       rq = group_req(g, g.gid[j]);
       if (HEADS) {
         act = g.act[j];
@@ -380,10 +387,12 @@ __global__ void __launch_bounds__(kBlock, MT_WRITE_MIN_BLOCKS_PER_SM) group_writ
     for (uint32_t q = 0; q < cnt; ++q) {
       const greq r = greq_shfl(t, rq, (int)q);
       const uint32_t* key = greq_key(g, r);
-      if constexpr (!HEADS) {
-        int res = RES_FAIL;
-        if (r.kind == MT_REQ_INSERT) res = coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
-        else if (r.kind == MT_REQ_UPDATE) res = coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
+      if constexpr (MODE == kGWInsert) {
+        const int res = coop_insert<T, false>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
+        if (t.leader() && r.d->results) r.d->results[r.i] = res == RES_OK;
+      } else if constexpr (MODE == kGWUpdErase) {
+        int res;
+        if (r.kind == MT_REQ_UPDATE) res = coop_update<T>(t, tv, cache, key, r.klen, greq_val(g, r), r.vlen);
         else res = coop_erase<T>(t, tv, key, r.klen);
         if (t.leader() && r.d->results) r.d->results[r.i] = res == RES_OK;
       } else {
@@ -459,7 +468,7 @@ int ensure_grouped(mt_masstree* t, uint32_t m, uint32_t max_v, cudaStream_t s) {
                                           hash_equal(), s) != cudaSuccess)
     return MT_ERR_CUDA;
   const size_t temp = std::max(sort_bytes, scan_bytes);
-  const size_t bytes = 4 * up256((size_t)m * 8u) + 2 * up256((size_t)m * sizeof(gfn)) + 7 * up256((size_t)m * 4u) +
+  const size_t bytes = 4 * up256((size_t)m * 8u) + 2 * up256((size_t)m * sizeof(gfn)) + 8 * up256((size_t)m * 4u) +
                        up256((size_t)m * max_v * 4u) + up256(temp);
   if (cudaDeviceSynchronize() != cudaSuccess) return MT_ERR_CUDA;
   if (t->grouped_mem) cudaFree(t->grouped_mem);
@@ -494,14 +503,15 @@ int launch_find_side(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
 }
 
 template <int TW>
-int launch_singles(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
-  int rc = launch_tile_kernel<TW>(t, group_write_kernel<TW, false>, g, s);
-  if (!rc) rc = launch_tile_kernel<TW>(t, group_serial_kernel<TW>, g, s);
+int launch_singles(mt_masstree* t, const grouped_view& g, cudaStream_t s_ins, cudaStream_t s_ue) {
+  int rc = launch_tile_kernel<TW>(t, group_write_kernel<TW, kGWInsert>, g, s_ins);
+  if (!rc) rc = launch_tile_kernel<TW>(t, group_write_kernel<TW, kGWUpdErase>, g, s_ue);
+  if (!rc) rc = launch_tile_kernel<TW>(t, group_serial_kernel<TW>, g, s_ue);
   return rc;
 }
 template <int TW>
 int launch_heads(mt_masstree* t, const grouped_view& g, cudaStream_t s) {
-  return launch_tile_kernel<TW>(t, group_write_kernel<TW, true>, g, s);
+  return launch_tile_kernel<TW>(t, group_write_kernel<TW, kGWHeads>, g, s);
 }
 
 }  // namespace
@@ -537,9 +547,10 @@ int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s) {
   g.singles = reinterpret_cast<uint32_t*>(carve(M * 4u));
   g.serial = reinterpret_cast<uint32_t*>(carve(M * 4u));
   g.finds = reinterpret_cast<uint32_t*>(carve(M * 4u));
+  g.singles_ue = reinterpret_cast<uint32_t*>(carve(M * 4u));
   void* temp = carve(t->grouped_temp);
   g.counts = b.status + 2;
-  if (cudaMemsetAsync(g.counts, 0, 4 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
+  if (cudaMemsetAsync(g.counts, 0, 5 * sizeof(uint32_t), s) != cudaSuccess) return MT_ERR_CUDA;
   const int grid = std::max(1, std::min<int>(t->sms * 8, (int)((m + 255u) / 256u)));
   group_hash_kernel<<<grid, 256, 0, s>>>(t->tv, g, hash_in, gid_in);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
@@ -562,7 +573,7 @@ int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s) {
   rc = host_fork(t, s);
   if (rc) return rc;
   const bool w16 = t->write_tile_size <= 16;
-  rc = w16 ? launch_singles<16>(t, g, t->side[0]) : launch_singles<32>(t, g, t->side[0]);
+  rc = w16 ? launch_singles<16>(t, g, t->side[0], t->side[1]) : launch_singles<32>(t, g, t->side[0], t->side[1]);
   if (!rc) {
     switch (t->tile_size) {
       case 4: rc = launch_find_side<4>(t, g, s); break;
