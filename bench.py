@@ -60,13 +60,17 @@ def parse():
     ap.add_argument("--cpu-batches", type=int, default=4, help="timed 1M-request batches in the CPU sample")
     ap.add_argument("--pool-gb", type=float, default=0.0,
                     help="slab pool size in GB (default: 60%% of the free device memory)")
+    ap.add_argument("--grouped-max-ops", type=int, default=1 << 20,
+                    help="largest sub-batch of the opt-in grouped section")
     ap.add_argument("--sections", default="batched,served,c1,c3",
-                    help="extra measurements at N=1: batched (256 sub-batches, tuned persistent launch from a "
+                    help="extra measurements at N=1: batched (256 sub-batches, tuned form replayed from a "
                          "CUDA graph, against one call per sub-batch), served (request loop over 64M keys, "
                          "latency against offered load, against one call per request), c1 (plain insert and "
                          "find, 1M keys), c3 (range scan, 32M keys); 'none' to skip; also space (slabs "
                          "held after erase rounds without merges, with merges, and with merges and emptied-"
-                         "layer removal; not in the default list)")
+                         "layer removal; not in the default list), grouped (one grouped mixed_batches call on "
+                         "--subbatches sub-batches of up to --grouped-max-ops requests: the profiling case of "
+                         "that form; not in the default list)")
     ap.add_argument("--space-keys", type=int, default=1 << 21, help="tree size for the space section")
     ap.add_argument("--subbatches", type=int, default=256)
     ap.add_argument("--tune-subbatches", type=int, default=16, help="sub-batches per autotuner trial")
@@ -335,6 +339,8 @@ def run_ours(args, rank, world, dist):
             extra["batched"] = run_batched(args, tree, c2, stream)
         if "served" in wanted:
             extra["served"] = run_served(args, tree, c2, stream)
+        if "grouped" in wanted:
+            extra["grouped"] = run_grouped(args, tree, c2, stream)
     tree.close()
     if world == 1 and ("c1" in wanted or "c3" in wanted):
         del tree
@@ -514,6 +520,40 @@ def run_batched(args, tree, c2, stream):
             "batched_over_per_call": round(batched / per_call, 3),
             "tuned": best, "trials": trials,
             "note": "each form runs its own draw of the ops (same sizes) on the live tree"}
+
+
+def run_grouped(args, tree, c2, stream):
+    """One grouped mt_mixed_batches call (MT_FLAG_GROUP_BY_KEY) on --subbatches
+    sub-batches of log-uniform sizes in [1K, --grouped-max-ops], after one untimed
+    call of a single find that sizes its scratch (opt-in section, the profiling
+    case of the grouped form)."""
+    import torch
+    from indexingpu_b200.masstree import pack_subbatches
+    st = wl.serve_stream(c2, args.subbatches, min_ops=1024, max_ops=args.grouped_max_ops, seed=0xC4, op_seed=0xC4,
+                         first_fresh=args.preload + (1 << 30))
+    dev = _dev_ops(torch, st)
+    desc = torch.from_numpy(pack_subbatches(_subbatches(dev, st))).cuda()
+    total = int(st["nops"].sum())
+    tree.set_tile_size(32)
+    tree.reserve_batches(args.subbatches, total)
+    one = dict(types=torch.full((1,), wl.REQ_FIND, dtype=torch.uint8, device="cuda"),
+               keys=torch.zeros((1, MAXK), dtype=torch.uint32, device="cuda"),
+               lens=torch.full((1,), MAXK, dtype=torch.uint32, device="cuda"),
+               vals=torch.zeros((1, MAXV), dtype=torch.uint32, device="cuda"),
+               vlens=torch.zeros(1, dtype=torch.uint32, device="cuda"), results=None, n=1)
+    tree.mixed_batches(torch.from_numpy(pack_subbatches([one])).cuda(), 1, MAXK, MAXV, stream=stream,
+                       group_by_key=True)
+    tree.sync(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tree.mixed_batches(desc, args.subbatches, MAXK, MAXV, stream=stream, group_by_key=True)
+    e1.record(stream)
+    tree.sync(stream)
+    ms = e0.elapsed_time(e1)
+    tree.set_tile_size(args.tile)
+    return {"workload": f"{args.subbatches} sub-batches of log-uniform sizes in [1K, {args.grouped_max_ops}], C2 mix",
+            "requests": total, "ms": round(ms, 3), "mops": round(total / ms / 1e3, 2),
+            "tiles": {"find": 32, "write": args.write_tile}}
 
 
 def run_served(args, tree, c2, stream):
