@@ -236,7 +236,8 @@ int mt_batches_reserve(mt_masstree* tree, uint32_t max_subbatches, uint64_t max_
  * final contents are those of one call per sub-batch.  Its first call (and
  * one after a larger mt_batches_reserve) allocates about 100 bytes per
  * reserved request plus 4 per reserved request and value slice (outside
- * graph capture), later calls launch a fixed sequence.  The batched
+ * graph capture; when that does not fit, the call is served in the default
+ * form), later calls launch a fixed sequence.  The batched
  * counterpart of the reference's per-call mixed_batch
  * (gpu_masstree.hpp:173-191). */
 int mt_mixed_batches(mt_masstree* tree, const mt_subbatch* subbatches, uint32_t num_subbatches,

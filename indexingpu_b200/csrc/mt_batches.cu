@@ -266,7 +266,10 @@ extern "C" int mt_mixed_batches(mt_masstree* t, const mt_subbatch* subbatches, u
   if (rc) return rc;
   batches_prepare_kernel<<<1, 256, 0, s>>>(b, t->tv.pool);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
-  if (flags & MT_FLAG_GROUP_BY_KEY) return launch_grouped(t, b, s);
+  if (flags & MT_FLAG_GROUP_BY_KEY) {
+    const int grc = launch_grouped(t, b, s);
+    if (grc != kGroupedUnavailable) return grc;
+  }
   batches_partition_kernel<<<t->sms * 4, 256, 0, s>>>(b);
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_CUDA;
   if (!(flags & MT_FLAG_PERSISTENT)) return launch_forked(t, b, s);

@@ -520,7 +520,11 @@ namespace mtb {
 
 int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s) {
   const uint32_t m = (uint32_t)t->batches_max_total;
+  // CUB counts items in int; without room for the scratch the caller serves
+  // the call in the forked form instead (nothing has been launched yet).
+  if (m > 0x7FFFFFFFu) return kGroupedUnavailable;
   int rc = ensure_grouped(t, m, b.max_value_length, s);
+  if (rc == MT_ERR_OOM) return kGroupedUnavailable;
   if (rc) return rc;
   grouped_view g{};
   g.b = b;

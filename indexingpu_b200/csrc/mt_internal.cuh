@@ -255,7 +255,9 @@ int host_launch_reclaim(mt_masstree* t, cudaStream_t s);
 int host_fork(mt_masstree* t, cudaStream_t s);
 int host_join(mt_masstree* t, cudaStream_t s, int rc);
 void host_pipe_free(mt_masstree* t);  // mt_host.cu
-int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s);  // mt_grouped.cu
+// mt_grouped.cu; kGroupedUnavailable: its scratch does not fit, nothing launched.
+constexpr int kGroupedUnavailable = -1001;
+int launch_grouped(mt_masstree* t, const batches_view& b, cudaStream_t s);
 int host_launch_insert(mt_masstree* t, const batch_args& a, bool upsert, cudaStream_t s);
 // Bulk build of a new tree's first layer (mt_bulk.cu): MT_OK, an error, or
 // kBulkDeclined when the batch does not suit it (insert it as usual).
