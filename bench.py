@@ -659,10 +659,23 @@ def run_c1(args, stream, peak):
     n, nf, mk, mv = len(d["keys"]), len(d["find_keys"]), d["maxK"], d["maxV"]
     out_v = torch.zeros((nf, mv), dtype=torch.uint32, device="cuda")
     out_l = torch.zeros(nf, dtype=torch.uint32, device="cuda")
-    with GpuMasstree(pool_bytes=2 << 30, tile_size=args.tile) as t:
+    # The insert into an empty tree is one call (the bulk build): untimed once on
+    # a small sample (kernels loaded on first use), then the median of three
+    # fresh trees.
+    with GpuMasstree(pool_bytes=256 << 20, tile_size=args.tile) as w:
+        w.set_write_tile_size(args.write_tile)
+        w.insert(k[:65536], mk, l[:65536], v[:65536], mv, vl[:65536], 65536, stream=stream)
+        w.sync(stream)
+    ins = []
+    for rep in range(3):
+        t = GpuMasstree(pool_bytes=2 << 30, tile_size=args.tile)
         t.set_write_tile_size(args.write_tile)
-        ins_ms = _timed(stream, lambda: t.insert(k, mk, l, v, mv, vl, n, stream=stream))
+        ins.append(_timed(stream, lambda: t.insert(k, mk, l, v, mv, vl, n, stream=stream)))
         t.sync(stream)
+        if rep < 2:
+            t.close()
+    ins_ms = sorted(ins)[1]
+    with t:
         find = lambda: t.find(fk, mk, fl, out_v, mv, out_l, nf, stream=stream)  # noqa: E731
         for _ in range(3):
             find()
@@ -678,7 +691,8 @@ def run_c1(args, stream, peak):
     fb = int((4 * L + 4 + np.where(d["find_hit"], 4 * mv + 4 + 256, 4 + 128)).sum())
     ach = fb / (find_ms / 1e3) / 1e9
     return {"workload": "1M distinct keys of 1-8 random slices, 2-slice values; 1M finds, 50% hits",
-            "insert_mops": round(n / ins_ms / 1e3, 2), "find_mops": round(nf / find_ms / 1e3, 2),
+            "insert_mops": round(n / ins_ms / 1e3, 2), "insert_ms_3_trees": [round(x, 3) for x in ins],
+            "find_mops": round(nf / find_ms / 1e3, 2),
             "find_hits": hits,
             "find_roofline": {"achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                               "frac": round(ach / peak, 4), "algorithmic_bytes": fb,
