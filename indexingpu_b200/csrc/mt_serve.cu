@@ -719,6 +719,7 @@ struct copy_pool {
 };
 
 constexpr uint64_t kPoolMinOps = 4096;     // rounds this large are copied by the pool
+constexpr int kUpStreams = 3;              // upload streams of the online server
 constexpr uint64_t kRoundMaxOps = 1u << 17;  // a round admits at most this many ops (then uploads)
 
 }  // namespace
@@ -748,7 +749,9 @@ struct mt_server {
   server_view sv{};
   int blocks = 0;
   size_t nwarps = 0;
-  cudaStream_t s_work = nullptr, s_up = nullptr;
+  cudaStream_t s_work = nullptr;
+  cudaStream_t s_up[kUpStreams] = {};    // uploads (pump only)
+  cudaEvent_t up_join[kUpStreams] = {};  // joins the upload streams into s_up[0]
   std::vector<cudaEvent_t> ev_pool;  // pump only
   std::unique_ptr<std::atomic<uint64_t>[]> rec_ticket;
   std::unique_ptr<std::atomic<uint32_t>[]> rec_done;
@@ -773,7 +776,10 @@ namespace {
 
 void server_free(mt_server* S) {
   if (S->s_work) cudaStreamSynchronize(S->s_work);
-  if (S->s_up) cudaStreamSynchronize(S->s_up);
+  for (cudaStream_t st : S->s_up)
+    if (st) cudaStreamSynchronize(st);
+  for (cudaEvent_t e : S->up_join)
+    if (e) cudaEventDestroy(e);
   for (auto e : S->ev_pool) cudaEventDestroy(e);
   if (S->dmem) cudaFree(S->dmem);
   for (void* h : {S->hmem, (void*)S->m_vals, (void*)S->m_vlens, (void*)S->m_results, (void*)S->ring,
@@ -782,7 +788,8 @@ void server_free(mt_server* S) {
   if (S->d_finished) cudaFree(S->d_finished);
   if (S->d_ctl) cudaFree(S->d_ctl);
   if (S->d_held) cudaFree(S->d_held);
-  for (cudaStream_t st : {S->s_work, S->s_up})
+  if (S->s_work) cudaStreamDestroy(S->s_work);
+  for (cudaStream_t st : S->s_up)
     if (st) cudaStreamDestroy(st);
   delete S;
 }
@@ -816,21 +823,34 @@ void server_stage(mt_server* S, const srv_request& r) {
   for (uint32_t o = 0; o < n; ++o) S->h_order[start[rank(r.types[o])]++] = off + o;
 }
 
-// Upload staging ops [lo, hi) (one contiguous run) on the upload stream.
+// Upload staging ops [lo, hi) (one contiguous run): the six fields' copies
+// spread over the upload streams, so that the copy engines take them side by
+// side (a small copy costs microseconds of set-up; six in a row on one stream
+// were most of a small request's upload time).
 int server_upload_range(mt_server* S, uint32_t lo, uint32_t hi) {
   if (hi <= lo) return MT_OK;
   const uint32_t K = S->cfg.max_key_length, V = S->cfg.max_value_length, n = hi - lo;
-  cudaStream_t s = S->s_up;
+  int k = 0;
   auto cp = [&](void* d, const void* h, size_t bytes) {
-    return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s) == cudaSuccess;
+    return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, S->s_up[k++ % kUpStreams]) == cudaSuccess;
   };
-  const bool ok = cp(S->d_types + lo, S->h_types + lo, n) &&
-                  cp(S->d_keys + (size_t)lo * K, S->h_keys + (size_t)lo * K, (size_t)n * K * 4u) &&
-                  cp(S->d_klens + lo, S->h_klens + lo, (size_t)n * 4u) &&
+  const bool ok = cp(S->d_keys + (size_t)lo * K, S->h_keys + (size_t)lo * K, (size_t)n * K * 4u) &&
                   cp(S->d_vals + (size_t)lo * V, S->h_vals + (size_t)lo * V, (size_t)n * V * 4u) &&
+                  cp(S->d_types + lo, S->h_types + lo, n) &&
+                  cp(S->d_klens + lo, S->h_klens + lo, (size_t)n * 4u) &&
                   cp(S->d_vlens + lo, S->h_vlens + lo, (size_t)n * 4u) &&
                   cp(S->d_order + lo, S->h_order + lo, (size_t)n * 4u);
   return ok ? MT_OK : MT_ERR_CUDA;
+}
+
+// The round's copies on every upload stream are done when this event, recorded
+// on the first stream after it waits for the others, has completed.
+int server_round_event(mt_server* S, cudaEvent_t ev) {
+  for (int k = 1; k < kUpStreams; ++k)
+    if (cudaEventRecord(S->up_join[k], S->s_up[k]) != cudaSuccess ||
+        cudaStreamWaitEvent(S->s_up[0], S->up_join[k], 0) != cudaSuccess)
+      return MT_ERR_CUDA;
+  return cudaEventRecord(ev, S->s_up[0]) == cudaSuccess ? MT_OK : MT_ERR_CUDA;
 }
 
 // Results of a completed request, from the mapped outputs to its buffers:
@@ -978,7 +998,8 @@ void server_pump(mt_server* S) {
       }
       if (!rc) rc = server_upload_range(S, run_lo, run_hi);
       round.ev = take_event();
-      if (!round.ev || cudaEventRecord(round.ev, S->s_up) != cudaSuccess) rc = MT_ERR_CUDA;
+      if (!round.ev) rc = MT_ERR_CUDA;
+      if (!rc) rc = server_round_event(S, round.ev);
       if (!rc) rounds.push_back(std::move(round));
     }
     // ---- publish uploaded rounds as work items --------------------------------
@@ -1088,7 +1109,7 @@ void server_pump(mt_server* S) {
   // The device loop leaves at the stop flag (or its launch's time budget).
   __atomic_store_n(S->stop, 1u, __ATOMIC_RELEASE);
   cudaStreamSynchronize(S->s_work);
-  cudaStreamSynchronize(S->s_up);
+  for (cudaStream_t st : S->s_up) cudaStreamSynchronize(st);
   for (auto& rd : rounds) S->ev_pool.push_back(rd.ev);
   for (auto e : evs) cudaEventDestroy(e);
   if (rc) S->status = rc;
@@ -1148,7 +1169,13 @@ extern "C" int mt_server_start(mt_masstree* t, const mt_server_config* cfg, mt_s
        cudaMalloc(&S->d_held, S->nwarps * sizeof(unsigned long long)) == cudaSuccess &&
        cudaMemset(S->d_held, 0xFF, S->nwarps * sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&S->s_work, cudaStreamNonBlocking) == cudaSuccess &&
-       cudaStreamCreateWithFlags(&S->s_up, cudaStreamNonBlocking) == cudaSuccess;
+       [&] {
+         for (int k = 0; k < kUpStreams; ++k)
+           if (cudaStreamCreateWithFlags(&S->s_up[k], cudaStreamNonBlocking) != cudaSuccess ||
+               cudaEventCreateWithFlags(&S->up_join[k], cudaEventDisableTiming) != cudaSuccess)
+             return false;
+         return true;
+       }();
   if (ok) {
     S->slots.resize(R);
     S->rec_ticket.reset(new (std::nothrow) std::atomic<uint64_t>[S->L]);
