@@ -147,6 +147,9 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) server_kernel(tr
   tile<T> t;
   slab_cache<T> cache;
   cache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / T);
+  tile<32> tw;
+  slab_cache<32> wcache;
+  if (T < 32) wcache.init(tv.pool, (blockIdx.x * blockDim.x + threadIdx.x) / 32u);
   constexpr uint32_t tiles_per_warp = 32u / T;
   const uint32_t tile_in_warp = lane / T;
   server_ctl* ctl = sv.ctl;
@@ -190,7 +193,17 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) server_kernel(tr
     a.n_dev = nullptr;
     a.n_back_dev = nullptr;
     a.n = it.count;
-    serve_requests<T, OP_MIXED, true>(t, tv, cache, a, tile_in_warp, tiles_per_warp);
+    // Items are cut from each request's ops in kind order (finds first): an
+    // item that starts with a write holds writes only, and the whole warp
+    // serves it as one 32-lane tile, the width writes run best at (as the
+    // write classes of a mixed batch); finds keep the narrow tiles.
+    uint32_t k0 = 0;
+    if (T < 32 && lane == 0 && it.count > 0u) k0 = a.types[a.index[0]];
+    if (T < 32 && __shfl_sync(0xFFFFFFFFu, k0, 0) != (uint32_t)MT_REQ_FIND) {
+      serve_requests<32, OP_MIXED, true>(tw, tv, wcache, a, 0u, 1u);
+    } else {
+      serve_requests<T, OP_MIXED, true>(t, tv, cache, a, tile_in_warp, tiles_per_warp);
+    }
     __syncwarp();
     if (lane == 0) {
       // acq_rel: the last item of a request has seen every write of the
@@ -214,6 +227,7 @@ __global__ void __launch_bounds__(kBlock, MT_MIN_BLOCKS_PER_SM) server_kernel(tr
   }
   if (lane == 0) sv.held[wid] = keep;
   cache.release(t, tv.pool);
+  if (T < 32) wcache.release(tw, tv.pool);
 }
 
 // Slabs handed out and not yet back on a free stack (in use + limbo), written
