@@ -100,10 +100,12 @@ def test_mixed_batches_match_per_call(tf, tw, bucket, persistent):
         new.close()
 
 
-@pytest.mark.parametrize("persistent", [False, True])
-def test_mixed_batches_graph_replay(persistent):
+@pytest.mark.parametrize("form", ["forked", "persistent", "grouped"])
+def test_mixed_batches_graph_replay(form):
     """Capture one mt_mixed_batches call in a CUDA graph, then replay it after
-    rewriting the sub-batch buffers in place with the next batches' data."""
+    rewriting the sub-batch buffers in place with the next batches' data (the
+    grouped form's scratch is sized by its first call, before the capture)."""
+    persistent, grouped = form == "persistent", form == "grouped"
     import torch
     c2 = wl.C2(n_preload=20000, n_prefixes=64)
     ref, new = _make_pair(torch, c2, 20000, 8, 32)
@@ -147,11 +149,11 @@ def test_mixed_batches_graph_replay(persistent):
         load(plans[0])
         s = torch.cuda.Stream()
         with torch.cuda.stream(s):
-            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent)
+            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent, group_by_key=grouped)
         new.sync(s)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=s):
-            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent)
+            new.mixed_batches(desc, len(bufs), MAXK, MAXV, stream=s, persistent=persistent, group_by_key=grouped)
         for r in range(1, rounds):
             load(plans[r])
             g.replay()
